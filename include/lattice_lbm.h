@@ -1,0 +1,250 @@
+/*
+ * lattice_lbm.h -- C ABI of the B200 (sm_100a) D3Q19 wind-tunnel solver.
+ *
+ * Drop-in replacement for the solver API of Lattice
+ * (MarcosAsh/Lattice_Fluid_Dynamics, simulation/lib/lbm.h).  Every function
+ * the reference declares keeps its name, argument order and meaning; the
+ * one GL type in that API (the GLuint returned by LBM_GetVelocityBuffer)
+ * becomes a CUDA device pointer.  A C caller written against lbm.h links
+ * this library in place of simulation/src/lbm.c; code that pokes the
+ * public LBMGrid fields (simulation/src/main.c:503-516,
+ * simulation/test/test_lbm.c:373,391-393) keeps compiling because those
+ * fields keep their names.
+ *
+ * Threading: one CUDA stream per grid.  LBM_Step only enqueues work; every
+ * function that returns data to the host synchronises that stream.  All
+ * functions are safe to call from one host thread per grid.
+ *
+ * Errors: functions keep the reference's return conventions (LBM_Create
+ * returns NULL, LBM_InitializeFlow returns 0, the void functions fail
+ * silently) and additionally record an LBM_ERR_* code readable with
+ * LBM_GetLastError.  No function traps the device.
+ */
+#ifndef LATTICE_LBM_H
+#define LATTICE_LBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Population storage formats (LBM_CreateEx).  FP16 and BF16 store the
+ * shifted deviation f_i - w_i and collide in FP32; FP64 stores and
+ * collides in double. */
+enum {
+    LBM_STORAGE_FP32 = 0,
+    LBM_STORAGE_FP16 = 1,
+    LBM_STORAGE_BF16 = 2,
+    LBM_STORAGE_FP64 = 3
+};
+
+enum {
+    LBM_OK = 0,
+    LBM_ERR_INVALID_ARGUMENT = 1,
+    LBM_ERR_OUT_OF_MEMORY = 2,
+    LBM_ERR_CUDA = 3,
+    LBM_ERR_NOT_INITIALIZED = 4,
+    LBM_ERR_UNSUPPORTED = 5,
+    LBM_ERR_DIVERGED = 6,
+    LBM_ERR_TIMEOUT = 7
+};
+
+/* Grid handle.  The first fields are the public scalars of the reference
+ * struct (simulation/lib/lbm.h:6-56) under the same names; callers may set
+ * tau and the operator flags between steps exactly as with the reference.
+ * The GL buffer/program/uniform fields of the reference have no
+ * counterpart; device state lives behind `impl`. */
+typedef struct LBMGrid {
+    int sizeX, sizeY, sizeZ;
+    int totalCells;
+    float tau;
+    int useRegularized;  /* 0 = BGK, 1 = regularized            */
+    int useMRT;          /* 1 = MRT (d'Humieres 2002) collision  */
+    int useSmagorinsky;  /* 1 = Smagorinsky SGS tau_eff          */
+    float smagorinskyCs; /* Smagorinsky constant                 */
+    int periodicYZ;      /* 0 = clamp, 1 = periodic y/z          */
+    /* extensions of this library */
+    int storage;         /* LBM_STORAGE_*, fixed at creation     */
+    int lastError;       /* last LBM_ERR_* code                  */
+    void *impl;          /* opaque device state                  */
+} LBMGrid;
+
+/* Particle record of the reference (simulation/lib/particle_system.h:12-17,
+ * shader struct particle_lbm.comp:4-9): 32 bytes. */
+typedef struct LBMParticle {
+    float x, y, z, pad;
+    float vx, vy, vz, life;
+} LBMParticle;
+
+/* ---------------------------------------------------------------------
+ * Reference API (simulation/lib/lbm.h:58-129)
+ * ------------------------------------------------------------------- */
+
+/* lbm.h:59 / lbm.c:46-318.  tau = 0.5 + 3*viscosity clamped to [0.52, 2];
+ * FP32 storage.  NULL on failure. */
+LBMGrid *LBM_Create(int sizeX, int sizeY, int sizeZ, float viscosity);
+
+/* lbm.h:62 / lbm.c:320-344.  Accepts NULL. */
+void LBM_Free(LBMGrid *grid);
+
+/* lbm.h:65-71 / lbm.c:346-435.  World box [-4,4]x[-2,2]x[-2,2]; q = 0.5 on
+ * every fluid->solid link. */
+void LBM_SetSolidAABB(LBMGrid *grid, float minX, float minY, float minZ,
+                      float maxX, float maxY, float maxZ);
+
+/* lbm.h:74 / lbm.c:670-721.  f = f_new = feq(1,u), velocity = (u,1).
+ * Returns 1 on success, 0 on failure. */
+int LBM_InitializeFlow(LBMGrid *grid, float ux, float uy, float uz);
+
+/* lbm.h:77 / lbm.c:723-821.  One collide + stream step (asynchronous). */
+void LBM_Step(LBMGrid *grid, float inletVelX, float inletVelY,
+              float inletVelZ);
+
+/* lbm.h:80 / lbm.c:823-825.  The reference returns the GL SSBO holding
+ * vec4(ux,uy,uz,rho) per cell; this returns the CUDA device pointer to the
+ * same float4 array (x-fastest, 16 bytes per cell), valid until the next
+ * LBM_Step / LBM_Free.  The stream is synchronised before returning. */
+const void *LBM_GetVelocityBuffer(LBMGrid *grid);
+
+/* lbm.h:83-86 / lbm.c:827-833 */
+void LBM_ComputeDragForce(LBMGrid *grid, float *forceX, float *forceY,
+                          float *forceZ);
+
+/* lbm.h:90-96 / lbm.c:835-918.  Mei-Luo-Shyy momentum exchange with the
+ * reference's per-cell x1e4 integer quantisation; pressure pointers may be
+ * NULL. */
+void LBM_ComputeDragForceDecomposed(LBMGrid *grid, float *forceX,
+                                    float *forceY, float *forceZ,
+                                    float *pressureX, float *pressureY,
+                                    float *pressureZ);
+
+/* lbm.h:99-101 / lbm.c:920-940: |Fx| / (0.5 U^2 A) */
+float LBM_ComputeDragCoefficient(LBMGrid *grid, float inletVelocity,
+                                 float refArea);
+
+/* lbm.h:104-106 / lbm.c:942-962: |Fy| / (0.5 U^2 A) */
+float LBM_ComputeLiftCoefficient(LBMGrid *grid, float inletVelocity,
+                                 float refArea);
+
+/* lbm.h:109-110 / lbm.c:437-535.  Analytic ray-sphere Bouzidi q. */
+void LBM_SetSolidSphere(LBMGrid *grid, float cx, float cy, float cz,
+                        float radius);
+
+/* lbm.h:114 / lbm.c:537-614.  Ground cells get solid = 2. */
+void LBM_AddGroundPlane(LBMGrid *grid, float worldZ);
+
+/* lbm.h:118 / lbm.c:616-668.  Count of (.,.) columns holding a solid==1
+ * cell along `axis` (0 = x, 1 = y, 2 = z). */
+float LBM_ComputeProjectedArea(LBMGrid *grid, int axis);
+
+/* lbm.h:121-129 / lbm.c:964-1223.  `triangles` holds 12 floats per
+ * triangle {v0,pad,v1,pad,v2,pad} (GPUTriangle, model_bounds.h:14-18);
+ * +x ray-parity fill inside the given box, Moller-Trumbore q per link. */
+void LBM_SetSolidMesh(LBMGrid *grid, float *triangles, int numTriangles,
+                      float minX, float minY, float minZ, float maxX,
+                      float maxY, float maxZ);
+
+/* simulation/lib/vti_export.h (vti_export.c:10-116): writes
+ * <path>/field_<step %06d>.vti with velocity, rho and solid. */
+void writeVTI(LBMGrid *grid, const char *path, int step);
+
+/* ---------------------------------------------------------------------
+ * Replacements for the reference's direct GL buffer access
+ * (main.c:1029, vti_export.c:30-34, test_lbm.c:258,503 read
+ * grid->solidBuffer / grid->velocityBuffer with glGetBufferSubData).
+ * All return 1 on success, 0 on failure, and synchronise the stream.
+ * ------------------------------------------------------------------- */
+
+/* float4 (ux,uy,uz,rho) per cell -> host[4*totalCells] */
+int LBM_CopyVelocity(LBMGrid *grid, float *host);
+/* int32 solid mask (0 fluid, 1 body, 2 ground) -> host[totalCells] */
+int LBM_CopySolid(LBMGrid *grid, int32_t *host);
+/* post-stream populations f in the reference's AoS order
+ * host[i + 19*cell]; FP64 grids convert to float */
+int LBM_CopyPopulations(LBMGrid *grid, float *host);
+/* post-collision populations f_new (the reference's fNewBuffer) */
+int LBM_CopyPostCollision(LBMGrid *grid, float *host);
+/* FP64 grids: both population arrays in double */
+int LBM_CopyPopulationsF64(LBMGrid *grid, double *host);
+int LBM_CopyPostCollisionF64(LBMGrid *grid, double *host);
+/* dense Bouzidi table q[i + 19*cell], -1 where there is no link (the
+ * reference's qBuffer) */
+int LBM_CopyQ(LBMGrid *grid, float *host);
+/* number of boundary links (entries with q >= 0) */
+long long LBM_GetBoundaryLinkCount(LBMGrid *grid);
+/* compacted boundary-link list sorted by (cell, direction); any of the
+ * three output pointers may be NULL */
+int LBM_CopyBoundaryLinks(LBMGrid *grid, int32_t *cell, int32_t *dir,
+                          float *q);
+/* device pointer of the grid's cudaStream_t */
+void *LBM_GetStream(LBMGrid *grid);
+
+/* ---------------------------------------------------------------------
+ * Extensions
+ * ------------------------------------------------------------------- */
+
+/* LBM_Create with a population storage format (LBM_STORAGE_*). */
+LBMGrid *LBM_CreateEx(int sizeX, int sizeY, int sizeZ, float viscosity,
+                      int storage);
+
+/* LBM_SetSolidSphere with q = 0.5 on every link (half-way bounce-back). */
+void LBM_SetSolidSphereHalfway(LBMGrid *grid, float cx, float cy, float cz,
+                               float radius);
+
+/* Run `nSteps` steps with a constant inlet velocity; launches are
+ * captured into a CUDA graph and replayed. */
+void LBM_StepN(LBMGrid *grid, int nSteps, float inletVelX, float inletVelY,
+               float inletVelZ);
+
+/* Force with FP64 accumulation (no quantisation): out[6] = fx,fy,fz,px,py,pz.
+ * Also returns the reference's int-quantised sums in raw7 (may be NULL):
+ * x,y,z,count,px,py,pz in units of 1e-4. */
+int LBM_ComputeDragForceF64(LBMGrid *grid, double *out6, long long *raw7);
+
+/* Global sums in FP64 over all cells of the post-stream state:
+ * out[0] = mass (sum of rho), out[1..3] = momentum. */
+int LBM_ComputeMassMomentum(LBMGrid *grid, double *out4);
+
+/* Cells reset by the stability guard since LBM_InitializeFlow. */
+long long LBM_GetGuardResetCount(LBMGrid *grid);
+
+/* Load post-stream populations (reference AoS order, float) as the new
+ * state; velocity is recomputed on demand.  Checkpoint restore. */
+int LBM_LoadPopulations(LBMGrid *grid, const float *host);
+
+/* Initialise from a macroscopic field: f = f_new = feq(rho, u) per cell,
+ * host arrays rho[totalCells], u[3*totalCells] (x-fastest). */
+int LBM_InitializeFromField(LBMGrid *grid, const float *rho, const float *u);
+
+/* Last error code of the grid (LBM_ERR_*), and a readable name. */
+int LBM_GetLastError(LBMGrid *grid);
+const char *LBM_GetErrorString(int code);
+
+/* Bytes of population traffic one lattice update moves (19 loads + 19
+ * stores of the storage type): 152 FP32, 76 FP16/BF16, 304 FP64. */
+int LBM_BytesPerUpdate(LBMGrid *grid);
+
+/* ---------------------------------------------------------------------
+ * Particles (particle_lbm.comp:46-89 trilinear sampler, :207-293 Euler
+ * step with collisionMode 0).  Particles live in device memory.
+ * ------------------------------------------------------------------- */
+typedef struct LBMParticles LBMParticles;
+
+/* n particles seeded uniformly on the inlet plane x = -4 (y, z uniform in
+ * [-2, 2)) by a counter hash of (seed, index); velocity 0, life 1. */
+LBMParticles *LBM_ParticlesCreate(int n, unsigned int seed);
+void LBM_ParticlesFree(LBMParticles *p);
+/* One Euler step of dt through the grid's current velocity field; runs on
+ * the grid's stream. */
+int LBM_ParticlesStep(LBMParticles *p, LBMGrid *grid, float dt);
+int LBM_ParticlesCopy(LBMParticles *p, LBMParticle *host);
+int LBM_ParticlesLoad(LBMParticles *p, const LBMParticle *host);
+/* device pointer to the LBMParticle array */
+void *LBM_ParticlesDevice(LBMParticles *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

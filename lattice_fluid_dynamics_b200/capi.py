@@ -1,0 +1,340 @@
+"""ctypes binding of the C ABI in include/lattice_lbm.h.
+
+This is the Python-side mirror of the reference's solver interface
+(simulation/lib/lbm.h): the same ``LBM_*`` entry points with the same
+argument meaning, plus the readback functions that replace the
+reference's direct GL buffer access.  The library is the in-tree
+``liblattice_lbm.so`` built by ``lattice_fluid_dynamics_b200.build``; there
+is no fallback -- loading fails loudly if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblattice_lbm.so")
+
+LBM_STORAGE_FP32 = 0
+LBM_STORAGE_FP16 = 1
+LBM_STORAGE_BF16 = 2
+LBM_STORAGE_FP64 = 3
+STORAGE_NAMES = {"fp32": 0, "fp16": 1, "bf16": 2, "fp64": 3}
+
+
+class LBMGrid(C.Structure):
+    """Mirror of ``struct LBMGrid`` (public fields of simulation/lib/lbm.h:6-56)."""
+    _fields_ = [
+        ("sizeX", C.c_int), ("sizeY", C.c_int), ("sizeZ", C.c_int),
+        ("totalCells", C.c_int),
+        ("tau", C.c_float),
+        ("useRegularized", C.c_int),
+        ("useMRT", C.c_int),
+        ("useSmagorinsky", C.c_int),
+        ("smagorinskyCs", C.c_float),
+        ("periodicYZ", C.c_int),
+        ("storage", C.c_int),
+        ("lastError", C.c_int),
+        ("impl", C.c_void_p),
+    ]
+
+
+class LBMParticle(C.Structure):
+    _fields_ = [(n, C.c_float) for n in
+                ("x", "y", "z", "pad", "vx", "vy", "vz", "life")]
+
+
+# every exported symbol with its (restype, argtypes)
+_G = C.POINTER(LBMGrid)
+_f = C.c_float
+_vp = C.c_void_p
+SIGNATURES = {
+    "LBM_Create": (_G, [C.c_int, C.c_int, C.c_int, _f]),
+    "LBM_CreateEx": (_G, [C.c_int, C.c_int, C.c_int, _f, C.c_int]),
+    "LBM_Free": (None, [_G]),
+    "LBM_SetSolidAABB": (None, [_G] + [_f] * 6),
+    "LBM_InitializeFlow": (C.c_int, [_G, _f, _f, _f]),
+    "LBM_Step": (None, [_G, _f, _f, _f]),
+    "LBM_StepN": (None, [_G, C.c_int, _f, _f, _f]),
+    "LBM_GetVelocityBuffer": (_vp, [_G]),
+    "LBM_ComputeDragForce": (None, [_G, _vp, _vp, _vp]),
+    "LBM_ComputeDragForceDecomposed": (None, [_G] + [_vp] * 6),
+    "LBM_ComputeDragCoefficient": (_f, [_G, _f, _f]),
+    "LBM_ComputeLiftCoefficient": (_f, [_G, _f, _f]),
+    "LBM_SetSolidSphere": (None, [_G, _f, _f, _f, _f]),
+    "LBM_SetSolidSphereHalfway": (None, [_G, _f, _f, _f, _f]),
+    "LBM_AddGroundPlane": (None, [_G, _f]),
+    "LBM_ComputeProjectedArea": (_f, [_G, C.c_int]),
+    "LBM_SetSolidMesh": (None, [_G, _vp, C.c_int] + [_f] * 6),
+    "writeVTI": (None, [_G, C.c_char_p, C.c_int]),
+    "LBM_CopyVelocity": (C.c_int, [_G, _vp]),
+    "LBM_CopySolid": (C.c_int, [_G, _vp]),
+    "LBM_CopyPopulations": (C.c_int, [_G, _vp]),
+    "LBM_CopyPostCollision": (C.c_int, [_G, _vp]),
+    "LBM_CopyPopulationsF64": (C.c_int, [_G, _vp]),
+    "LBM_CopyPostCollisionF64": (C.c_int, [_G, _vp]),
+    "LBM_CopyQ": (C.c_int, [_G, _vp]),
+    "LBM_GetBoundaryLinkCount": (C.c_longlong, [_G]),
+    "LBM_CopyBoundaryLinks": (C.c_int, [_G, _vp, _vp, _vp]),
+    "LBM_GetStream": (_vp, [_G]),
+    "LBM_ComputeDragForceF64": (C.c_int, [_G, _vp, _vp]),
+    "LBM_ComputeMassMomentum": (C.c_int, [_G, _vp]),
+    "LBM_GetGuardResetCount": (C.c_longlong, [_G]),
+    "LBM_LoadPopulations": (C.c_int, [_G, _vp]),
+    "LBM_InitializeFromField": (C.c_int, [_G, _vp, _vp]),
+    "LBM_GetLastError": (C.c_int, [_G]),
+    "LBM_GetErrorString": (C.c_char_p, [C.c_int]),
+    "LBM_BytesPerUpdate": (C.c_int, [_G]),
+    "LBM_ParticlesCreate": (_vp, [C.c_int, C.c_uint]),
+    "LBM_ParticlesFree": (None, [_vp]),
+    "LBM_ParticlesStep": (C.c_int, [_vp, _G, _f]),
+    "LBM_ParticlesCopy": (C.c_int, [_vp, _vp]),
+    "LBM_ParticlesLoad": (C.c_int, [_vp, _vp]),
+    "LBM_ParticlesDevice": (_vp, [_vp]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load the solver library (no fallback: raises if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise RuntimeError(
+                f"{path} is missing: build it with "
+                "`python -m lattice_fluid_dynamics_b200.build`")
+        lib = C.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class Grid:
+    """One solver grid.  Method names follow the reference's C API."""
+
+    def __init__(self, nx: int, ny: int, nz: int, viscosity: float,
+                 storage: int | str = LBM_STORAGE_FP32):
+        self._L = load()
+        if isinstance(storage, str):
+            storage = STORAGE_NAMES[storage]
+        self._g = self._L.LBM_CreateEx(nx, ny, nz, viscosity, storage)
+        if not self._g:
+            raise RuntimeError(f"LBM_CreateEx({nx},{ny},{nz}) failed")
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.n = nx * ny * nz
+        self.storage = storage
+
+    # -- lifetime --
+    def close(self):
+        if getattr(self, "_g", None):
+            self._L.LBM_Free(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- public struct fields --
+    @property
+    def s(self) -> LBMGrid:
+        return self._g.contents
+
+    def set(self, **kw):
+        for k, v in kw.items():
+            setattr(self._g.contents, k, v)
+        return self
+
+    @property
+    def tau(self) -> float:
+        return self.s.tau
+
+    @property
+    def handle(self):
+        return self._g
+
+    def check(self):
+        err = self._L.LBM_GetLastError(self._g)
+        if err != 0:
+            raise RuntimeError("LBM error: " + self._L.LBM_GetErrorString(err).decode())
+
+    # -- reference API --
+    def set_solid_aabb(self, minX, minY, minZ, maxX, maxY, maxZ):
+        self._L.LBM_SetSolidAABB(self._g, minX, minY, minZ, maxX, maxY, maxZ)
+        self.check()
+
+    def set_solid_sphere(self, cx, cy, cz, r, halfway=False):
+        fn = self._L.LBM_SetSolidSphereHalfway if halfway else self._L.LBM_SetSolidSphere
+        fn(self._g, cx, cy, cz, r)
+        self.check()
+
+    def add_ground_plane(self, z):
+        self._L.LBM_AddGroundPlane(self._g, z)
+        self.check()
+
+    def set_solid_mesh(self, tris: np.ndarray, bbox):
+        tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 12)
+        self._L.LBM_SetSolidMesh(self._g, _p(tris), tris.shape[0], *bbox)
+        self.check()
+
+    def projected_area(self, axis=0) -> float:
+        return self._L.LBM_ComputeProjectedArea(self._g, axis)
+
+    def initialize_flow(self, ux, uy=0.0, uz=0.0):
+        if self._L.LBM_InitializeFlow(self._g, ux, uy, uz) != 1:
+            self.check()
+            raise RuntimeError("LBM_InitializeFlow failed")
+
+    def initialize_from_field(self, rho: np.ndarray, u: np.ndarray):
+        rho = np.ascontiguousarray(rho, np.float32).reshape(-1)
+        u = np.ascontiguousarray(u, np.float32).reshape(-1, 3)
+        if self._L.LBM_InitializeFromField(self._g, _p(rho), _p(u)) != 1:
+            self.check()
+            raise RuntimeError("LBM_InitializeFromField failed")
+
+    def step(self, ux, uy=0.0, uz=0.0, n: int = 1):
+        if n == 1:
+            self._L.LBM_Step(self._g, ux, uy, uz)
+        else:
+            self._L.LBM_StepN(self._g, n, ux, uy, uz)
+
+    def step_loop(self, ux, uy=0.0, uz=0.0, n: int = 1):
+        for _ in range(n):
+            self._L.LBM_Step(self._g, ux, uy, uz)
+
+    def drag_force_decomposed(self) -> np.ndarray:
+        out = (C.c_float * 6)()
+        self._L.LBM_ComputeDragForceDecomposed(
+            self._g, *[C.addressof(out) + 4 * k for k in range(6)])
+        self.check()
+        return np.frombuffer(out, np.float32).copy()
+
+    def drag_force_f64(self):
+        out = np.zeros(6, np.float64)
+        raw = np.zeros(7, np.int64)
+        if not self._L.LBM_ComputeDragForceF64(self._g, _p(out), _p(raw)):
+            self.check()
+        return out, raw
+
+    def drag_coefficient(self, U, A) -> float:
+        return self._L.LBM_ComputeDragCoefficient(self._g, U, A)
+
+    def lift_coefficient(self, U, A) -> float:
+        return self._L.LBM_ComputeLiftCoefficient(self._g, U, A)
+
+    def velocity_device_ptr(self) -> int:
+        return self._L.LBM_GetVelocityBuffer(self._g)
+
+    def stream_ptr(self) -> int:
+        return self._L.LBM_GetStream(self._g)
+
+    def write_vti(self, path: str, step: int):
+        self._L.writeVTI(self._g, path.encode(), step)
+
+    # -- readbacks --
+    def velocity(self) -> np.ndarray:
+        out = np.empty((self.n, 4), np.float32)
+        assert self._L.LBM_CopyVelocity(self._g, _p(out)) == 1
+        return out
+
+    def solid(self) -> np.ndarray:
+        out = np.empty(self.n, np.int32)
+        assert self._L.LBM_CopySolid(self._g, _p(out)) == 1
+        return out
+
+    def populations(self) -> np.ndarray:
+        out = np.empty((self.n, 19), np.float32)
+        assert self._L.LBM_CopyPopulations(self._g, _p(out)) == 1
+        return out
+
+    def post_collision(self) -> np.ndarray:
+        out = np.empty((self.n, 19), np.float32)
+        assert self._L.LBM_CopyPostCollision(self._g, _p(out)) == 1
+        return out
+
+    def populations_f64(self) -> np.ndarray:
+        out = np.empty((self.n, 19), np.float64)
+        assert self._L.LBM_CopyPopulationsF64(self._g, _p(out)) == 1
+        return out
+
+    def post_collision_f64(self) -> np.ndarray:
+        out = np.empty((self.n, 19), np.float64)
+        assert self._L.LBM_CopyPostCollisionF64(self._g, _p(out)) == 1
+        return out
+
+    def q(self) -> np.ndarray:
+        out = np.empty((self.n, 19), np.float32)
+        assert self._L.LBM_CopyQ(self._g, _p(out)) == 1
+        return out
+
+    def links(self):
+        nl = self._L.LBM_GetBoundaryLinkCount(self._g)
+        cell = np.empty(nl, np.int32)
+        d = np.empty(nl, np.int32)
+        q = np.empty(nl, np.float32)
+        assert self._L.LBM_CopyBoundaryLinks(self._g, _p(cell), _p(d), _p(q)) == 1
+        return cell, d, q
+
+    def load_populations(self, f: np.ndarray):
+        f = np.ascontiguousarray(f, np.float32).reshape(self.n, 19)
+        assert self._L.LBM_LoadPopulations(self._g, _p(f)) == 1
+
+    def mass_momentum(self) -> np.ndarray:
+        out = np.zeros(4, np.float64)
+        assert self._L.LBM_ComputeMassMomentum(self._g, _p(out)) == 1
+        return out
+
+    def guard_resets(self) -> int:
+        return int(self._L.LBM_GetGuardResetCount(self._g))
+
+    def bytes_per_update(self) -> int:
+        return int(self._L.LBM_BytesPerUpdate(self._g))
+
+
+class Particles:
+    def __init__(self, n: int, seed: int = 0):
+        self._L = load()
+        self._p = self._L.LBM_ParticlesCreate(n, seed)
+        if not self._p:
+            raise RuntimeError("LBM_ParticlesCreate failed")
+        self.n = n
+
+    def close(self):
+        if getattr(self, "_p", None):
+            self._L.LBM_ParticlesFree(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, grid: Grid, dt: float):
+        assert self._L.LBM_ParticlesStep(self._p, grid.handle, dt) == 1
+
+    def get(self) -> np.ndarray:
+        out = np.empty((self.n, 8), np.float32)
+        assert self._L.LBM_ParticlesCopy(self._p, _p(out)) == 1
+        return out
+
+    def set(self, arr: np.ndarray):
+        arr = np.ascontiguousarray(arr, np.float32).reshape(self.n, 8)
+        assert self._L.LBM_ParticlesLoad(self._p, _p(arr)) == 1

@@ -1,0 +1,81 @@
+// Storage-format dispatch of the step kernels (instantiated in
+// lbm_step_{f32,f64,f16,bf16}.cu).
+#include "lbm_step.cuh"
+
+namespace lbm {
+
+extern template struct StepLaunch<StoreF32>;
+extern template struct StepLaunch<StoreF64>;
+extern template struct StepLaunch<StoreF16>;
+extern template struct StepLaunch<StoreBF16>;
+
+#define LBM_DISPATCH(storage, CALL)                               \
+    switch (storage) {                                            \
+        case LBM_STORAGE_FP32: return StepLaunch<StoreF32>::CALL; \
+        case LBM_STORAGE_FP64: return StepLaunch<StoreF64>::CALL; \
+        case LBM_STORAGE_FP16: return StepLaunch<StoreF16>::CALL; \
+        case LBM_STORAGE_BF16: return StepLaunch<StoreBF16>::CALL; \
+        default: return cudaErrorInvalidValue;                    \
+    }
+
+cudaError_t launch_step(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
+                        cudaStream_t s) {
+    LBM_DISPATCH(g.storage, step(g, a, fused, op, smag, s));
+}
+
+static StepArgs stream_args(const GridImpl &g, const void *src, void *dst, int periodic) {
+    StepArgs a{};
+    a.src = src;
+    a.dst = dst;
+    a.flags = g.flags;
+    a.slot = g.slot;
+    a.bmask = g.links.bmask;
+    a.bfirst = g.links.bfirst;
+    a.lq = g.links.lq;
+    a.nx = g.nx;
+    a.ny = g.ny;
+    a.nz = g.nz;
+    a.n = g.n;
+    a.periodic = periodic;
+    return a;
+}
+
+cudaError_t launch_stream_only(const GridImpl &g, const void *src, void *dst, int periodic,
+                               cudaStream_t s) {
+    StepArgs a = stream_args(g, src, dst, periodic);
+    LBM_DISPATCH(g.storage, stream_only(g, a, s));
+}
+
+cudaError_t launch_velocity(const GridImpl &g, const void *src, int kind, int periodic,
+                            float inX, float inY, float inZ, float4 *vel, cudaStream_t s) {
+    StepArgs a = stream_args(g, src, nullptr, periodic);
+    a.inX = inX;
+    a.inY = inY;
+    a.inZ = inZ;
+    LBM_DISPATCH(g.storage, velocity(g, a, kind, vel, s));
+}
+
+cudaError_t launch_init_uniform(const GridImpl &g, void *a, void *b, float ux, float uy,
+                                float uz, cudaStream_t s) {
+    LBM_DISPATCH(g.storage, init_uniform(g, a, b, ux, uy, uz, s));
+}
+
+cudaError_t launch_init_field(const GridImpl &g, void *a, void *b, const float *rho,
+                              const float *u, cudaStream_t s) {
+    LBM_DISPATCH(g.storage, init_field(g, a, b, rho, u, s));
+}
+
+cudaError_t launch_export_aos(const GridImpl &g, const void *src, void *dst, bool as_double,
+                              cudaStream_t s) {
+    LBM_DISPATCH(g.storage, export_aos(g, src, dst, as_double, s));
+}
+
+cudaError_t launch_import_aos(const GridImpl &g, const float *src, void *dst, cudaStream_t s) {
+    LBM_DISPATCH(g.storage, import_aos(g, src, dst, s));
+}
+
+cudaError_t launch_mass_momentum(const GridImpl &g, const void *f, double *out4, cudaStream_t s) {
+    LBM_DISPATCH(g.storage, mass_momentum(g, f, out4, s));
+}
+
+}  // namespace lbm

@@ -1,0 +1,139 @@
+// Internal device state of an LBMGrid and the launchers shared by the
+// translation units of the library.  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/lattice_lbm.h"
+
+namespace lbm {
+
+// collision operators (lbm_collide.comp:488-625)
+enum { OP_BGK = 0, OP_REG = 1, OP_MRT = 2 };
+
+// Compacted boundary-link structure.  A boundary cell is a cell owning at
+// least one link with q >= 0 (the reference's dense q table entry for
+// (cell, dir)).  Links are stored sorted by (cell, dir); a boundary cell b
+// owns links [first[b], first[b+1]) and `mask[b]` has bit d set for each
+// linked direction d, so the link of direction d is
+// first[b] + popc(mask[b] & ((1 << d) - 1)).
+struct LinkList {
+    int nb = 0;              // boundary cells
+    long long nl = 0;        // links
+    int32_t *bcell = nullptr;   // [nb]
+    uint32_t *bmask = nullptr;  // [nb]
+    int32_t *bfirst = nullptr;  // [nb + 1]
+    float *lq = nullptr;        // [nl]
+    int32_t *lcell = nullptr;   // [nl]
+    int32_t *ldir = nullptr;    // [nl]
+};
+
+// What the population buffers hold.
+//   - `g` (index gbuf) always holds post-collision populations f_new.
+//   - When fbuf >= 0, buffer fbuf holds explicit post-stream f; otherwise
+//     f is implicit: f = Stream(g) with the links and periodic flag of the
+//     step that produced g.
+//   - The velocity field of the last step is derived from that step's
+//     input (buffer `vin`, kind `vin_kind`) until it is materialised in
+//     `vel` (vel_valid).
+enum InputKind { IN_EXPLICIT_F = 0, IN_POST_COLLISION = 1 };
+
+struct GridImpl {
+    int nx = 0, ny = 0, nz = 0;
+    long long n = 0;
+    int storage = LBM_STORAGE_FP32;
+    size_t elem = 4;          // bytes per stored population
+    cudaStream_t stream = nullptr;
+
+    void *pop[2] = {nullptr, nullptr};  // SoA planes pop[i * n + cell]
+    float4 *vel = nullptr;
+    int32_t *solid = nullptr;
+    uint8_t *flags = nullptr;
+    int32_t *slot = nullptr;            // boundary-cell index or -1
+    LinkList links;
+
+    long long *force_i64 = nullptr;     // [7]
+    double *force_f64 = nullptr;        // [6]
+    double *sums_f64 = nullptr;         // [4]
+    unsigned long long *guard = nullptr;  // cumulative guard resets
+    int *err_flag = nullptr;            // device-side error word
+    long long *host_pinned = nullptr;   // small pinned readback area (64 B)
+
+    bool initialized = false;
+    int gbuf = 1;
+    int fbuf = 0;             // -1 when f is implicit
+    int stream_periodic = 0;  // periodic flag of the stream that turns g into f
+    bool vel_valid = true;
+    int vin = 0;
+    int vin_kind = IN_EXPLICIT_F;
+    int vin_periodic = 0;     // periodic flag of the stream feeding vin (post-collision kind)
+    float vin_inlet[3] = {0, 0, 0};
+
+    // launch configuration of the step kernel (autotuned)
+    int bx = 128, by = 1;
+
+    // CUDA graphs for LBM_StepN, one per starting buffer parity (gbuf)
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int graph_key[2][8] = {{0}, {0}};
+};
+
+struct StepArgs {
+    const void *src;   // populations read (post-collision g or explicit f)
+    void *dst;         // populations written (post-collision)
+    const uint8_t *flags;
+    const int32_t *slot;
+    const uint32_t *bmask;
+    const int32_t *bfirst;
+    const float *lq;
+    int nx, ny, nz;
+    long long n;
+    int periodic;      // periodic flag of the stream part
+    float tau, omega, smagCs;
+    float inX, inY, inZ;
+    unsigned long long *guard;
+};
+
+// lbm_step.cu
+cudaError_t launch_step(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
+                        cudaStream_t s);
+cudaError_t launch_stream_only(const GridImpl &g, const void *src, void *dst, int periodic,
+                               cudaStream_t s);
+cudaError_t launch_velocity(const GridImpl &g, const void *src, int kind, int periodic,
+                            float inX, float inY, float inZ, float4 *vel, cudaStream_t s);
+cudaError_t launch_init_uniform(const GridImpl &g, void *a, void *b, float ux, float uy,
+                                float uz, cudaStream_t s);
+cudaError_t launch_init_field(const GridImpl &g, void *a, void *b, const float *rho,
+                              const float *u, cudaStream_t s);
+cudaError_t launch_export_aos(const GridImpl &g, const void *src, void *dst, bool as_double,
+                              cudaStream_t s);
+cudaError_t launch_import_aos(const GridImpl &g, const float *src, void *dst, cudaStream_t s);
+cudaError_t launch_mass_momentum(const GridImpl &g, const void *f_explicit, double *out4,
+                                 cudaStream_t s);
+
+// lbm_geometry.cu
+cudaError_t geo_fill_q(float *qd, long long n19, cudaStream_t s);
+cudaError_t geo_links_to_dense(const GridImpl &g, float *qd, cudaStream_t s);
+cudaError_t geo_aabb(GridImpl &g, float *qd, float minX, float minY, float minZ, float maxX,
+                     float maxY, float maxZ, cudaStream_t s);
+cudaError_t geo_sphere(GridImpl &g, float *qd, float cx, float cy, float cz, float r,
+                       bool halfway, cudaStream_t s);
+cudaError_t geo_ground(GridImpl &g, float *qd, float worldZ, cudaStream_t s);
+cudaError_t geo_mesh(GridImpl &g, float *qd, const float *tris_dev, int ntris,
+                     const float bbox[6], cudaStream_t s);
+cudaError_t geo_compact(GridImpl &g, const float *qd, cudaStream_t s);
+cudaError_t geo_projected_area(const GridImpl &g, int axis, int *count_dev, cudaStream_t s);
+void geo_free_links(LinkList &l);
+
+// lbm_force.cu
+cudaError_t launch_force(const GridImpl &g, const void *gsrc, const void *f_explicit,
+                         int periodic, const float4 *vel_or_null, const void *vin_src,
+                         int vin_kind, int vin_periodic, const float vin_inlet[3],
+                         long long *i64, double *f64, cudaStream_t s);
+
+// lbm_particles.cu
+cudaError_t launch_particles(LBMParticle *p, int n, const float4 *vel, int nx, int ny, int nz,
+                             float dt, uint32_t seed, cudaStream_t s);
+void particles_seed_host(LBMParticle *p, int n, uint32_t seed);
+
+}  // namespace lbm

@@ -1,0 +1,335 @@
+// Step kernels of the D3Q19 solver, templated on the population storage
+// format.  Included by one .cu file per storage format so the template
+// instantiations compile in parallel.
+//
+// Layout in HBM: populations are SoA planes, pop[i * n + cell] with
+// cell = x + NX * (y + NY * z); one plane per direction, two full copies
+// (ping-pong).  A warp covers 32 consecutive x of one row, so every load
+// of a plane is a 128-byte coalesced access (shifted by one element for
+// the directions with e_x != 0) and every store is aligned.
+//
+// The fused kernel performs the reference's stream of step n
+// (lbm_stream.comp:76-129, including Bouzidi interpolated bounce-back on
+// the compacted boundary-link list) followed by the collision of step n+1
+// (lbm_collide.comp:313-626), reading post-collision populations and
+// writing post-collision populations: 2 x 19 population transfers and a
+// one-byte cell flag per lattice update.
+#pragma once
+
+#include "lbm_d3q19.cuh"
+#include "lbm_internal.h"
+
+namespace lbm {
+
+// Pull-stream gather of the post-stream populations of one cell from the
+// post-collision field `src` (lbm_stream.comp:85-128).
+template <class S>
+__device__ __forceinline__ void gather_stream(const StepArgs &a, const typename S::T *__restrict__ src,
+                                              int x, int y, int z, long long cell, uint8_t flag,
+                                              typename S::R (&f)[19]) {
+    using R = typename S::R;
+    const long long n = a.n;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    int ym = y - 1, yp = y + 1, zm = z - 1, zp = z + 1;
+    if (a.periodic == 1) {
+        if (ym < 0) ym += ny;
+        if (yp >= ny) yp -= ny;
+        if (zm < 0) zm += nz;
+        if (zp >= nz) zp -= nz;
+    } else {
+        ym = ym < 0 ? 0 : ym;
+        yp = yp > ny - 1 ? ny - 1 : yp;
+        zm = zm < 0 ? 0 : zm;
+        zp = zp > nz - 1 ? nz - 1 : zp;
+    }
+    const long long plane = (long long)nx * ny;
+    const long long rowY[3] = {(long long)ym * nx, (long long)y * nx, (long long)yp * nx};
+    const long long rowZ[3] = {(long long)zm * plane, (long long)z * plane, (long long)zp * plane};
+
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        const int sx = x - cx(i);
+        const long long sidx =
+            (sx < 0 || sx >= nx) ? cell : rowY[1 - cy(i)] + rowZ[1 - cz(i)] + sx;
+        f[i] = S::load(src + (long long)i * n + sidx, i);
+    }
+
+    if (flag & FLAG_BOUNDARY) {
+        const int b = a.slot[cell];
+        const uint32_t mask = a.bmask[b];
+        const int first = a.bfirst[b];
+#pragma unroll
+        for (int i = 0; i < 19; i++) {
+            const int io = opp(i);
+            if (mask & (1u << io)) {
+                const float q = a.lq[first + __popc(mask & ((1u << io) - 1u))];
+                const R fiopp = S::load(src + (long long)io * n + cell, io);
+                const R qq = R(q);
+                if (q >= 0.5f) {
+                    const R fi = S::load(src + (long long)i * n + cell, i);
+                    const R inv2q = ddiv<R>(R(1), R(2) * qq);
+                    f[i] = inv2q * fiopp + (R(1) - inv2q) * fi;
+                } else {
+                    const int fx = x + cx(i);
+                    R ff;
+                    if (fx >= 0 && fx < nx)
+                        ff = S::load(src + (long long)io * n + rowY[1 + cy(i)] +
+                                         rowZ[1 + cz(i)] + fx,
+                                     io);
+                    else
+                        ff = fiopp;
+                    const R twoq = R(2) * qq;
+                    f[i] = twoq * fiopp + (R(1) - twoq) * ff;
+                }
+            }
+        }
+    }
+}
+
+template <class S, int OP, bool SMAG, bool FUSED>
+__global__ void __launch_bounds__(256) k_step(const StepArgs a) {
+    using T = typename S::T;
+    using R = typename S::R;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= a.nx || y >= a.ny) return;
+    const long long n = a.n;
+    const long long cell = (long long)x + (long long)a.nx * ((long long)y + (long long)a.ny * z);
+    const uint8_t flag = a.flags[cell];
+    const T *__restrict__ src = static_cast<const T *>(a.src);
+    T *__restrict__ dst = static_cast<T *>(a.dst);
+
+    R f[19];
+    if (FUSED) {
+        gather_stream<S>(a, src, x, y, z, cell, flag, f);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 19; i++) f[i] = S::load(src + (long long)i * n + cell, i);
+    }
+
+    R rho, ux, uy, uz;
+    const int kind = prepare_cell<R>(f, flag & FLAG_SOLID_MASK, x, a.nx, R(a.inX), R(a.inY),
+                                     R(a.inZ), rho, ux, uy, uz);
+    R fn[19];
+    if (kind == 1) {
+#pragma unroll
+        for (int i = 0; i < 19; i++) fn[i] = f[opp(i)];
+    } else if (kind == 2) {
+#pragma unroll
+        for (int i = 0; i < 19; i++) fn[i] = feq<R>(i, R(1), R(0), R(0), R(0));
+    } else {
+        collide<R, OP, SMAG>(f, fn, rho, ux, uy, uz, R(a.tau), R(a.omega), R(a.smagCs));
+    }
+    const unsigned reset = __ballot_sync(__activemask(), kind == 2);
+    if (reset && (threadIdx.x & 31) == (unsigned)(__ffs(reset) - 1))
+        atomicAdd(a.guard, (unsigned long long)__popc(reset));
+#pragma unroll
+    for (int i = 0; i < 19; i++) S::store(dst + (long long)i * n + cell, fn[i], i);
+}
+
+// Stream only: materialise the post-stream populations f = Stream(g).
+template <class S>
+__global__ void __launch_bounds__(256) k_stream_only(const StepArgs a) {
+    using T = typename S::T;
+    using R = typename S::R;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= a.nx || y >= a.ny) return;
+    const long long n = a.n;
+    const long long cell = (long long)x + (long long)a.nx * ((long long)y + (long long)a.ny * z);
+    R f[19];
+    gather_stream<S>(a, static_cast<const T *>(a.src), x, y, z, cell, a.flags[cell], f);
+    T *dst = static_cast<T *>(a.dst);
+#pragma unroll
+    for (int i = 0; i < 19; i++) S::store(dst + (long long)i * n + cell, f[i], i);
+}
+
+// Velocity/density of a step (lbm_collide.comp:322-443): the moments of the
+// step's input after the solid rule, Zou-He and the guard.
+template <class S>
+__global__ void __launch_bounds__(256) k_velocity(const StepArgs a, int kind_in, float4 *vel) {
+    using T = typename S::T;
+    using R = typename S::R;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= a.nx || y >= a.ny) return;
+    const long long n = a.n;
+    const long long cell = (long long)x + (long long)a.nx * ((long long)y + (long long)a.ny * z);
+    const uint8_t flag = a.flags[cell];
+    const T *src = static_cast<const T *>(a.src);
+    R f[19];
+    if (kind_in == IN_POST_COLLISION) {
+        gather_stream<S>(a, src, x, y, z, cell, flag, f);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 19; i++) f[i] = S::load(src + (long long)i * n + cell, i);
+    }
+    R rho, ux, uy, uz;
+    prepare_cell<R>(f, flag & FLAG_SOLID_MASK, x, a.nx, R(a.inX), R(a.inY), R(a.inZ), rho, ux,
+                    uy, uz);
+    vel[cell] = make_float4(float(ux), float(uy), float(uz), float(rho));
+}
+
+// Uniform equilibrium initialisation (lbm.c:670-721) of both buffers.
+template <class S>
+__global__ void k_init_uniform(typename S::T *a, typename S::T *b, long long n, float ux,
+                               float uy, float uz) {
+    using R = typename S::R;
+    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= n) return;
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        const R e = feq<R>(i, R(1), R(ux), R(uy), R(uz));
+        S::store(a + (long long)i * n + cell, e, i);
+        S::store(b + (long long)i * n + cell, e, i);
+    }
+}
+
+template <class S>
+__global__ void k_init_field(typename S::T *a, typename S::T *b, long long n,
+                             const float *__restrict__ rho, const float *__restrict__ u) {
+    using R = typename S::R;
+    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= n) return;
+    const R r = R(rho[cell]);
+    const R ux = R(u[3 * cell]), uy = R(u[3 * cell + 1]), uz = R(u[3 * cell + 2]);
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        const R e = feq<R>(i, r, ux, uy, uz);
+        S::store(a + (long long)i * n + cell, e, i);
+        S::store(b + (long long)i * n + cell, e, i);
+    }
+}
+
+// SoA storage -> AoS float/double in the reference order f[i + 19*cell]
+template <class S, typename O>
+__global__ void k_export_aos(const typename S::T *__restrict__ src, O *__restrict__ dst,
+                             long long n) {
+    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= n) return;
+#pragma unroll
+    for (int i = 0; i < 19; i++) dst[19 * cell + i] = O(S::load(src + (long long)i * n + cell, i));
+}
+
+template <class S>
+__global__ void k_import_aos(const float *__restrict__ src, typename S::T *__restrict__ dst,
+                             long long n) {
+    using R = typename S::R;
+    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= n) return;
+#pragma unroll
+    for (int i = 0; i < 19; i++) S::store(dst + (long long)i * n + cell, R(src[19 * cell + i]), i);
+}
+
+// FP64 mass and momentum of explicit post-stream populations.
+template <class S>
+__global__ void __launch_bounds__(256) k_mass_momentum(const typename S::T *__restrict__ f,
+                                                        long long n, double *out4) {
+    double acc[4] = {0, 0, 0, 0};
+    for (long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x; cell < n;
+         cell += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int i = 0; i < 19; i++) {
+            const double v = double(S::load(f + (long long)i * n + cell, i));
+            acc[0] += v;
+            acc[1] += double(cx(i)) * v;
+            acc[2] += double(cy(i)) * v;
+            acc[3] += double(cz(i)) * v;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        double v = acc[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(out4 + k, v);
+    }
+}
+
+// ---------------------------------------------------------------------
+// Host-side launchers for one storage format
+// ---------------------------------------------------------------------
+template <class S>
+struct StepLaunch {
+    static dim3 grid3(const GridImpl &g) {
+        return dim3((g.nx + g.bx - 1) / g.bx, (g.ny + g.by - 1) / g.by, g.nz);
+    }
+
+    template <int OP, bool SMAG>
+    static void go(const GridImpl &g, const StepArgs &a, bool fused, cudaStream_t s) {
+        const dim3 blk(g.bx, g.by, 1);
+        if (fused)
+            k_step<S, OP, SMAG, true><<<grid3(g), blk, 0, s>>>(a);
+        else
+            k_step<S, OP, SMAG, false><<<grid3(g), blk, 0, s>>>(a);
+    }
+
+    static cudaError_t step(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
+                            cudaStream_t s) {
+        switch (op * 2 + (smag ? 1 : 0)) {
+            case 0: go<OP_BGK, false>(g, a, fused, s); break;
+            case 1: go<OP_BGK, true>(g, a, fused, s); break;
+            case 2: go<OP_REG, false>(g, a, fused, s); break;
+            case 3: go<OP_REG, true>(g, a, fused, s); break;
+            case 4: go<OP_MRT, false>(g, a, fused, s); break;
+            default: go<OP_MRT, true>(g, a, fused, s); break;
+        }
+        return cudaGetLastError();
+    }
+
+    static cudaError_t stream_only(const GridImpl &g, const StepArgs &a, cudaStream_t s) {
+        k_stream_only<S><<<grid3(g), dim3(g.bx, g.by, 1), 0, s>>>(a);
+        return cudaGetLastError();
+    }
+
+    static cudaError_t velocity(const GridImpl &g, const StepArgs &a, int kind, float4 *vel,
+                                cudaStream_t s) {
+        k_velocity<S><<<grid3(g), dim3(g.bx, g.by, 1), 0, s>>>(a, kind, vel);
+        return cudaGetLastError();
+    }
+
+    static cudaError_t init_uniform(const GridImpl &g, void *a, void *b, float ux, float uy,
+                                    float uz, cudaStream_t s) {
+        const unsigned blocks = (unsigned)((g.n + 255) / 256);
+        k_init_uniform<S><<<blocks, 256, 0, s>>>(static_cast<typename S::T *>(a),
+                                                 static_cast<typename S::T *>(b), g.n, ux, uy, uz);
+        return cudaGetLastError();
+    }
+
+    static cudaError_t init_field(const GridImpl &g, void *a, void *b, const float *rho,
+                                  const float *u, cudaStream_t s) {
+        const unsigned blocks = (unsigned)((g.n + 255) / 256);
+        k_init_field<S><<<blocks, 256, 0, s>>>(static_cast<typename S::T *>(a),
+                                               static_cast<typename S::T *>(b), g.n, rho, u);
+        return cudaGetLastError();
+    }
+
+    static cudaError_t export_aos(const GridImpl &g, const void *src, void *dst, bool as_double,
+                                  cudaStream_t s) {
+        const unsigned blocks = (unsigned)((g.n + 255) / 256);
+        if (as_double)
+            k_export_aos<S, double><<<blocks, 256, 0, s>>>(
+                static_cast<const typename S::T *>(src), static_cast<double *>(dst), g.n);
+        else
+            k_export_aos<S, float><<<blocks, 256, 0, s>>>(
+                static_cast<const typename S::T *>(src), static_cast<float *>(dst), g.n);
+        return cudaGetLastError();
+    }
+
+    static cudaError_t import_aos(const GridImpl &g, const float *src, void *dst, cudaStream_t s) {
+        const unsigned blocks = (unsigned)((g.n + 255) / 256);
+        k_import_aos<S><<<blocks, 256, 0, s>>>(src, static_cast<typename S::T *>(dst), g.n);
+        return cudaGetLastError();
+    }
+
+    static cudaError_t mass_momentum(const GridImpl &g, const void *f, double *out4,
+                                     cudaStream_t s) {
+        k_mass_momentum<S><<<148 * 8, 256, 0, s>>>(static_cast<const typename S::T *>(f), g.n,
+                                                   out4);
+        return cudaGetLastError();
+    }
+};
+
+}  // namespace lbm

@@ -1,0 +1,6 @@
+// Step-kernel instantiations for StoreBF16 populations.
+#include "lbm_step.cuh"
+
+namespace lbm {
+template struct StepLaunch<StoreBF16>;
+}  // namespace lbm

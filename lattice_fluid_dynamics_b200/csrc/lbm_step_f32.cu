@@ -1,0 +1,6 @@
+// Step-kernel instantiations for StoreF32 populations.
+#include "lbm_step.cuh"
+
+namespace lbm {
+template struct StepLaunch<StoreF32>;
+}  // namespace lbm

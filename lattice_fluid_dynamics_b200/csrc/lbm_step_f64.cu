@@ -1,0 +1,6 @@
+// Step-kernel instantiations for StoreF64 populations.
+#include "lbm_step.cuh"
+
+namespace lbm {
+template struct StepLaunch<StoreF64>;
+}  // namespace lbm

@@ -1,0 +1,346 @@
+"""GPU parity: the CUDA library (through its C ABI) against the CPU oracle on
+the same seeded inputs.
+
+Bar (from the hot-path contract): solid masks and boundary-link lists
+bit-exact; populations within 1e-5 relative; Cd/Cl within 1e-4 relative.
+The FP32 kernels are built to perform the oracle's exact rounding
+sequence, so the tests also report (and mostly require) exact equality.
+"""
+import numpy as np
+import pytest
+
+from tests import scenarios as S
+
+pytestmark = pytest.mark.gpu
+
+POP_RTOL = 1e-5      # populations, relative
+CD_RTOL = 1e-4       # drag / lift coefficients, relative
+
+
+def _assert_links_equal(og, gg):
+    oc, od, oq = og.links()
+    gc, gd, gq = gg.links()
+    assert oc.shape == gc.shape, (oc.shape, gc.shape)
+    np.testing.assert_array_equal(gc, oc)
+    np.testing.assert_array_equal(gd, od)
+    np.testing.assert_array_equal(gq.view(np.uint32), oq.view(np.uint32))
+
+
+def _assert_state_close(og, gg, rtol=POP_RTOL):
+    f_o, f_g = og.f, gg.populations()
+    fn_o, fn_g = og.f_new, gg.post_collision()
+    v_o, v_g = og.vel, gg.velocity()
+    assert S.rel_err(f_g, f_o) <= rtol, S.rel_err(f_g, f_o)
+    assert S.rel_err(fn_g, fn_o) <= rtol, S.rel_err(fn_g, fn_o)
+    np.testing.assert_allclose(v_g, v_o, rtol=rtol, atol=1e-7)
+    return float(np.mean(f_g == f_o))
+
+
+# --------------------------------------------------------------------------
+# geometry: masks and link lists bit-exact
+# --------------------------------------------------------------------------
+GEOMETRIES = {
+    "box16": ((16, 8, 8), [S.BOX]),
+    "box_ground32": ((32, 16, 16), [S.BOX, ("ground", (-0.15,))]),
+    "sphere_c1": ((128, 64, 64), [S.sphere_c1()]),
+    "sphere_halfway_c1": ((128, 64, 64), [S.sphere_c1(halfway=True)]),
+    "sphere_re100": ((128, 64, 64), [("sphere", (0.0, 0.0, 0.0, 0.5))]),
+    "aabb_then_sphere": ((48, 24, 24), [S.BOX, ("sphere", (0.3, 0.1, -0.1, 0.4))]),
+}
+
+
+@pytest.mark.parametrize("name", sorted(GEOMETRIES))
+def test_masks_and_links_bitexact(oracle, solver, name):
+    dims, geo = GEOMETRIES[name]
+    sc = dict(dims=dims, geometry=geo)
+    og = S.make_oracle(oracle, sc)
+    gg = S.make_gpu(solver, sc)
+    np.testing.assert_array_equal(gg.solid(), og.solid)
+    _assert_links_equal(og, gg)
+    np.testing.assert_array_equal(gg.q().view(np.uint32), og.q.view(np.uint32))
+    for axis in range(3):
+        assert gg.projected_area(axis) == og.projected_area(axis)
+
+
+def test_mesh_uv_sphere_bitexact(oracle, solver):
+    from lattice_fluid_dynamics_b200 import geometry as G
+    tris, bbox = G.uv_sphere(0.6, center=(-1.0, 0.05, -0.02), n_theta=24, n_phi=32)
+    sc = dict(dims=(64, 32, 32), geometry=[("mesh", (tris, bbox))])
+    og = S.make_oracle(oracle, sc)
+    gg = S.make_gpu(solver, sc)
+    assert og.solid.sum() > 0
+    np.testing.assert_array_equal(gg.solid(), og.solid)
+    _assert_links_equal(og, gg)
+
+
+def test_mesh_ahmed_c2_bitexact(oracle, solver):
+    """Config 2 geometry: the 19,800-triangle Ahmed-style body at 256x128x128."""
+    from lattice_fluid_dynamics_b200 import geometry as G
+    tris, bbox = G.ahmed_body()
+    sc = dict(dims=(256, 128, 128), visc=1e-4, geometry=[("mesh", (tris, bbox))])
+    og = S.make_oracle(oracle, sc)
+    gg = S.make_gpu(solver, sc)
+    assert og.solid.sum() > 20000
+    np.testing.assert_array_equal(gg.solid(), og.solid)
+    _assert_links_equal(og, gg)
+    assert gg.projected_area(0) == og.projected_area(0)
+
+
+# --------------------------------------------------------------------------
+# dynamics: every collision operator / boundary mode against the oracle
+# --------------------------------------------------------------------------
+OPS = [
+    dict(),
+    dict(useRegularized=1),
+    dict(useMRT=1),
+    dict(useSmagorinsky=1, smagorinskyCs=0.1),
+    dict(useRegularized=1, useSmagorinsky=1, smagorinskyCs=0.17),
+    dict(useMRT=1, useSmagorinsky=1, smagorinskyCs=0.1),
+]
+
+
+@pytest.mark.parametrize("periodic", [0, 1])
+@pytest.mark.parametrize("opi", range(len(OPS)))
+def test_operators_match_oracle(oracle, solver, opi, periodic):
+    flags = dict(OPS[opi], periodicYZ=periodic)
+    sc = dict(dims=(40, 20, 16), visc=0.02, flags=flags,
+              geometry=[("sphere", (-1.0, 0.1, -0.05, 0.45)), ("ground", (-1.6,))])
+    og = S.make_oracle(oracle, sc)
+    gg = S.make_gpu(solver, sc)
+    for _ in range(3):
+        og.step(0.06, 0.01, -0.005, n=20)
+        gg.step(0.06, 0.01, -0.005, n=20)
+        exact = _assert_state_close(og, gg)
+        assert exact == 1.0, f"populations not bit-identical ({exact:.6f} equal)"
+        fo = og.drag_force_decomposed()
+        fg = gg.drag_force_decomposed()
+        np.testing.assert_array_equal(fg, fo)
+        assert og.force_raw == list(gg.drag_force_f64()[1])
+
+
+def test_box_1000_steps_reference_test(oracle, solver):
+    """simulation/test/test_lbm.c:271-301 on both sides: nonzero drag after
+    10 and 1000 steps, 0 < Cd < 1000 with A = 4, and GPU == oracle."""
+    sc = dict(dims=(16, 8, 8), visc=0.1, geometry=[S.BOX])
+    og = S.make_oracle(oracle, sc)
+    gg = S.make_gpu(solver, sc)
+    og.step(0.05, n=10)
+    gg.step(0.05, n=10)
+    fo, fg = og.drag_force_decomposed(), gg.drag_force_decomposed()
+    assert abs(fg[0]) > 1e-10
+    np.testing.assert_array_equal(fg, fo)
+    og.step(0.05, n=990)
+    gg.step(0.05, n=990)
+    _assert_state_close(og, gg)
+    cd_o, cd_g = og.drag_coefficient(0.05, 4.0), gg.drag_coefficient(0.05, 4.0)
+    assert 0 < cd_g < 1000
+    assert abs(cd_g - cd_o) <= CD_RTOL * abs(cd_o)
+
+
+@pytest.mark.parametrize("halfway", [True, False])
+def test_config1_sphere_1000_steps(oracle, solver, halfway):
+    """Config 1: 128x64x64 BGK FP32, tau = 0.6, u_in = (0.05, 0, 0), sphere
+    r = 8 cells at lattice cell (32,32,32); Cd/Cl every 10 steps for 1000
+    steps; populations after 1000 steps."""
+    sc = dict(dims=(128, 64, 64), visc=(0.6 - 0.5) / 3, tau=0.6,
+              geometry=[S.sphere_c1(halfway)])
+    og = S.make_oracle(oracle, sc)
+    gg = S.make_gpu(solver, sc)
+    A = og.projected_area(0)
+    assert gg.projected_area(0) == A
+    worst = 0.0
+    for k in range(100):
+        og.step(0.05, n=10)
+        gg.step(0.05, n=10)
+        cd_o, cd_g = og.drag_coefficient(0.05, A), gg.drag_coefficient(0.05, A)
+        fo, fg = og.drag_force_decomposed(), gg.drag_force_decomposed()
+        cl_o = fo[1] / (0.5 * 0.05 * 0.05 * A)
+        cl_g = fg[1] / (0.5 * 0.05 * 0.05 * A)
+        worst = max(worst, abs(cd_g - cd_o) / max(abs(cd_o), 1e-12))
+        assert abs(cd_g - cd_o) <= CD_RTOL * abs(cd_o), (k, cd_g, cd_o)
+        assert abs(cl_g - cl_o) <= CD_RTOL * max(abs(cl_o), 1e-6), (k, cl_g, cl_o)
+    exact = _assert_state_close(og, gg)
+    print(f"config1 halfway={halfway}: Cd={cd_g:.6f} worst Cd rel err {worst:.2e}, "
+          f"populations bit-identical fraction {exact:.6f}")
+
+
+def test_config2_ahmed_mrt_smagorinsky(oracle, solver):
+    """Config 2 (first 100 steps): Ahmed-style body at 256x128x128,
+    MRT + Smagorinsky Cs = 0.1, tau from Re = 5e4 set directly, periodic y/z
+    as simulation/src/main.c:503-516 sets it; Cd, Cl and the pressure part
+    every 10 steps."""
+    from lattice_fluid_dynamics_b200 import geometry as G
+    tris, bbox = G.ahmed_body()
+    tau = G.reynolds_tau(0.05, 64.0, 5e4)
+    sc = dict(dims=(256, 128, 128), visc=1e-4, tau=tau,
+              flags=dict(useMRT=1, useSmagorinsky=1, smagorinskyCs=0.1, periodicYZ=1),
+              geometry=[("mesh", (tris, bbox))])
+    og = S.make_oracle(oracle, sc)
+    gg = S.make_gpu(solver, sc)
+    A = og.projected_area(0)
+    for _ in range(10):
+        og.step(0.05, n=10)
+        gg.step(0.05, n=10)
+        fo, fg = og.drag_force_decomposed(), gg.drag_force_decomposed()
+        np.testing.assert_allclose(fg, fo, rtol=CD_RTOL, atol=1e-4)
+    _assert_state_close(og, gg)
+    assert gg.drag_coefficient(0.05, A) > 0
+
+
+# --------------------------------------------------------------------------
+# the state machine behind the fused kernel
+# --------------------------------------------------------------------------
+def test_readback_does_not_perturb(oracle, solver):
+    sc = dict(dims=(32, 16, 16), visc=0.05, flags=dict(useMRT=1, periodicYZ=1),
+              geometry=[("sphere", (-1.5, 0.0, 0.0, 0.6))])
+    a = S.make_gpu(solver, sc)
+    b = S.make_gpu(solver, sc)
+    for k in range(30):
+        a.step(0.05)
+        b.step(0.05)
+        if k % 7 == 3:
+            a.populations()
+            a.velocity()
+            a.drag_force_decomposed()
+            a.mass_momentum()
+    np.testing.assert_array_equal(a.populations(), b.populations())
+    np.testing.assert_array_equal(a.velocity(), b.velocity())
+
+
+def test_geometry_change_mid_run_and_flag_toggle(oracle, solver):
+    sc = dict(dims=(32, 16, 16), visc=0.05, flags=dict(useMRT=1),
+              geometry=[S.BOX])
+    og = S.make_oracle(oracle, sc)
+    gg = S.make_gpu(solver, sc)
+    og.step(0.05, n=15)
+    gg.step(0.05, n=15)
+    og.add_ground_plane(-1.0)
+    gg.add_ground_plane(-1.0)
+    np.testing.assert_array_equal(gg.solid(), og.solid)
+    _assert_links_equal(og, gg)
+    og.set(periodicYZ=1)
+    gg.set(periodicYZ=1)
+    og.step(0.05, n=5)
+    gg.step_loop(0.05, n=5)
+    og.set(periodicYZ=0, useRegularized=1)
+    gg.set(periodicYZ=0, useRegularized=1)
+    og.step(0.04, n=7)
+    gg.step_loop(0.04, n=7)
+    _assert_state_close(og, gg)
+    np.testing.assert_array_equal(gg.drag_force_decomposed(), og.drag_force_decomposed())
+
+
+def test_stepn_graph_equals_step_loop(solver):
+    sc = dict(dims=(48, 24, 24), visc=0.05, flags=dict(useMRT=1, useSmagorinsky=1),
+              geometry=[("sphere", (-1.0, 0.0, 0.0, 0.5))])
+    a = S.make_gpu(solver, sc)
+    b = S.make_gpu(solver, sc)
+    a.step(0.05, n=101)          # graph path (chunks of 32 + remainder)
+    b.step_loop(0.05, n=101)
+    np.testing.assert_array_equal(a.populations(), b.populations())
+    a.step(0.05, n=64)
+    b.step_loop(0.05, n=64)
+    np.testing.assert_array_equal(a.post_collision(), b.post_collision())
+    np.testing.assert_array_equal(a.velocity(), b.velocity())
+
+
+def test_load_populations_checkpoint(solver):
+    sc = dict(dims=(24, 12, 12), visc=0.05, geometry=[S.BOX])
+    a = S.make_gpu(solver, sc)
+    a.step(0.05, n=20)
+    f = a.populations()
+    b = S.make_gpu(solver, sc)
+    b.load_populations(f)
+    np.testing.assert_array_equal(b.populations(), f)
+    a.step(0.05, n=10)
+    b.step(0.05, n=10)
+    np.testing.assert_array_equal(a.populations(), b.populations())
+
+
+def test_guard_resets_counted(oracle, solver):
+    """Stability guard (lbm_collide.comp:429-440): an unstable run resets the
+    same cells on both sides."""
+    sc = dict(dims=(24, 12, 12), visc=0.0, tau=0.5005,
+              geometry=[S.BOX], init=(0.3, 0.0, 0.0))
+    og = S.make_oracle(oracle, sc)
+    gg = S.make_gpu(solver, sc)
+    og.step(0.35, n=40)
+    gg.step_loop(0.35, n=40)
+    assert og.guard_resets > 0
+    assert gg.guard_resets() == og.guard_resets
+    _assert_state_close(og, gg)
+
+
+def test_mass_momentum_fp64(oracle, solver):
+    sc = dict(dims=(32, 16, 16), visc=0.05, flags=dict(periodicYZ=1), geometry=[S.BOX])
+    og = S.make_oracle(oracle, sc)
+    gg = S.make_gpu(solver, sc)
+    og.step(0.05, n=25)
+    gg.step(0.05, n=25)
+    f = og.f.astype(np.float64)
+    ref = np.array([f.sum(), (f[:, [1, 7, 9, 11, 13]].sum() - f[:, [2, 8, 10, 12, 14]].sum()),
+                    (f[:, [3, 7, 8, 15, 17]].sum() - f[:, [4, 9, 10, 16, 18]].sum()),
+                    (f[:, [5, 11, 12, 15, 16]].sum() - f[:, [6, 13, 14, 17, 18]].sum())])
+    np.testing.assert_allclose(gg.mass_momentum(), ref, rtol=1e-12, atol=1e-9)
+
+
+# --------------------------------------------------------------------------
+# precision variants against the FP64 oracle
+# --------------------------------------------------------------------------
+def test_fp64_storage_matches_fp64_oracle(oracle, solver):
+    sc = dict(dims=(32, 16, 16), visc=0.03, flags=dict(useMRT=1, useSmagorinsky=1),
+              geometry=[("sphere", (-1.5, 0.0, 0.0, 0.6))])
+    og = S.make_oracle(oracle, sc, prec=8)
+    gg = S.make_gpu(solver, sc, storage="fp64")
+    og.step(0.05, n=50)
+    gg.step(0.05, n=50)
+    fo = og.f
+    fg = gg.populations_f64()
+    assert S.rel_err(fg, fo) < 1e-12
+    out, raw = gg.drag_force_f64()
+    og.drag_force_decomposed()
+    np.testing.assert_allclose(out, og.force_f64, rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("storage,tol", [("fp16", 2e-3), ("bf16", 2e-2)])
+def test_reduced_precision_close_to_fp64(oracle, solver, storage, tol):
+    sc = dict(dims=(48, 24, 24), visc=0.02, flags=dict(useMRT=1),
+              geometry=[("sphere", (-1.5, 0.0, 0.0, 0.6))])
+    og = S.make_oracle(oracle, sc, prec=8)
+    gg = S.make_gpu(solver, sc, storage=storage)
+    og.step(0.05, n=100)
+    gg.step(0.05, n=100)
+    vo = og.vel[:, :3].astype(np.float64)
+    vg = gg.velocity()[:, :3].astype(np.float64)
+    l2 = np.linalg.norm(vg - vo) / np.linalg.norm(vo)
+    print(f"{storage}: relative L2 velocity error vs FP64 oracle = {l2:.3e}")
+    assert l2 < tol
+
+
+# --------------------------------------------------------------------------
+# consumers of the velocity field
+# --------------------------------------------------------------------------
+def test_particles_match_oracle(oracle, solver):
+    sc = dict(dims=(64, 32, 32), visc=0.05, geometry=[S.BOX])
+    gg = S.make_gpu(solver, sc)
+    gg.step(0.05, n=50)
+    vel = gg.velocity()
+    n, seed, dt = 50000, 0, 0.016
+    p = solver.Particles(n, seed)
+    ref = oracle.particles_seed_inlet(n, seed)
+    np.testing.assert_array_equal(p.get(), ref)
+    for _ in range(200):
+        p.step(gg, dt)
+        oracle.particles_step(vel, (64, 32, 32), ref, dt, seed)
+    np.testing.assert_array_equal(p.get(), ref)
+
+
+def test_write_vti_matches_reference_format(oracle, solver, tmp_path):
+    sc = dict(dims=(16, 8, 8), visc=0.1, geometry=[S.BOX])
+    gg = S.make_gpu(solver, sc)
+    gg.step(0.05, n=5)
+    gg.write_vti(str(tmp_path), 5)
+    got = (tmp_path / "field_000005.vti").read_bytes()
+    ref_path = str(tmp_path / "ref.vti")
+    assert oracle.write_vti(ref_path, (16, 8, 8), gg.velocity(), gg.solid())
+    assert got == open(ref_path, "rb").read()
