@@ -29,7 +29,7 @@ struct LBMParticles {
     int n = 0;
     uint32_t seed = 0;
     LBMParticle *dev = nullptr;
-    cudaStream_t last = nullptr;  // stream of the last step (synchronised before copies)
+    cudaEvent_t done = nullptr;  // recorded after each step on the grid's stream
 };
 
 namespace {
@@ -54,12 +54,20 @@ size_t elem_size(int storage) {
     }
 }
 
+// Step launch shape: 256-thread blocks of 32 x 8 cells (a warp spans 32
+// consecutive x), at least 4 blocks resident per SM (<= 64 registers).
+// Measured on B200 at 256x128x128 against 64x4 / 128x2 / 256x1 shapes and
+// an unconstrained register budget.  LBM_BLOCK=<bx>x<by>, LBM_MINB=1|4 and
+// LBM_CPT=1|2 override it.
 void default_block(GridImpl &I) {
-    int bx = 32;
-    while (bx < I.nx && bx < 128) bx *= 2;
-    I.bx = bx;
-    I.by = 256 / bx;
-    if (I.by > I.ny) I.by = I.ny < 1 ? 1 : I.ny;
+    I.bx = 32;
+    I.by = 8;
+    I.cpt = 1;
+    I.minb = 4;
+    const char *cenv = getenv("LBM_CPT");
+    if (cenv) I.cpt = atoi(cenv) == 2 ? 2 : 1;
+    const char *menv = getenv("LBM_MINB");
+    if (menv) I.minb = atoi(menv) == 1 ? 1 : 4;
     const char *env = getenv("LBM_BLOCK");
     if (env) {
         int a = 0, b = 0;
@@ -70,14 +78,19 @@ void default_block(GridImpl &I) {
     }
 }
 
-__global__ void k_fill_vel(float4 *v, long long n, float4 val) {
+__global__ void k_fill_vel(float4 *v, double4 *v64, long long n, float4 val) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) v[i] = val;
+    if (i >= n) return;
+    v[i] = val;
+    if (v64) v64[i] = make_double4(val.x, val.y, val.z, val.w);
 }
 
-__global__ void k_vel_from_field(float4 *v, long long n, const float *rho, const float *u) {
+__global__ void k_vel_from_field(float4 *v, double4 *v64, long long n, const float *rho,
+                                 const float *u) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) v[i] = make_float4(u[3 * i], u[3 * i + 1], u[3 * i + 2], rho[i]);
+    if (i >= n) return;
+    v[i] = make_float4(u[3 * i], u[3 * i + 1], u[3 * i + 2], rho[i]);
+    if (v64) v64[i] = make_double4(u[3 * i], u[3 * i + 1], u[3 * i + 2], rho[i]);
 }
 
 void drop_graph(GridImpl &I) {
@@ -94,7 +107,7 @@ bool ensure_vel(LBMGrid *grid) {
     GridImpl &I = *IMPL(grid);
     if (I.vel_valid) return true;
     if (!ok(grid, launch_velocity(I, I.pop[I.vin], I.vin_kind, I.vin_periodic, I.vin_inlet[0],
-                                  I.vin_inlet[1], I.vin_inlet[2], I.vel, I.stream)))
+                                  I.vin_inlet[1], I.vin_inlet[2], I.vel, I.vel64, I.stream)))
         return false;
     I.vel_valid = true;
     return true;
@@ -124,8 +137,11 @@ StepArgs step_args(LBMGrid *grid, GridImpl &I, float inX, float inY, float inZ) 
     a.nz = I.nz;
     a.n = I.n;
     a.tau = grid->tau;
+    // lbm_collide.comp:480-486 in each arithmetic precision
     a.omega = 1.0f / grid->tau;
-    a.smagCs = grid->smagorinskyCs;
+    a.smag18 = 18.0f * (grid->smagorinskyCs * grid->smagorinskyCs);
+    a.omega_d = 1.0 / (double)grid->tau;
+    a.smag18_d = 18.0 * ((double)grid->smagorinskyCs * (double)grid->smagorinskyCs);
     a.inX = inX;
     a.inY = inY;
     a.inZ = inZ;
@@ -263,6 +279,8 @@ LBMGrid *LBM_CreateEx(int sizeX, int sizeY, int sizeZ, float viscosity, int stor
     good = good && ok(grid, cudaMalloc(&I->pop[0], popBytes));
     good = good && ok(grid, cudaMalloc(&I->pop[1], popBytes));
     good = good && ok(grid, cudaMalloc(&I->vel, sizeof(float4) * (size_t)n));
+    if (storage == LBM_STORAGE_FP64)
+        good = good && ok(grid, cudaMalloc(&I->vel64, sizeof(double4) * (size_t)n));
     good = good && ok(grid, cudaMalloc(&I->solid, sizeof(int32_t) * (size_t)n));
     good = good && ok(grid, cudaMalloc(&I->flags, (size_t)n));
     good = good && ok(grid, cudaMalloc(&I->slot, sizeof(int32_t) * (size_t)n));
@@ -309,6 +327,7 @@ void LBM_Free(LBMGrid *grid) {
         cudaFree(I->pop[0]);
         cudaFree(I->pop[1]);
         cudaFree(I->vel);
+        cudaFree(I->vel64);
         cudaFree(I->solid);
         cudaFree(I->flags);
         cudaFree(I->slot);
@@ -403,7 +422,7 @@ int LBM_InitializeFlow(LBMGrid *grid, float ux, float uy, float uz) {
     drop_graph(*I);
     bool good = ok(grid, launch_init_uniform(*I, I->pop[0], I->pop[1], ux, uy, uz, I->stream));
     k_fill_vel<<<(unsigned)((I->n + 255) / 256), 256, 0, I->stream>>>(
-        I->vel, I->n, make_float4(ux, uy, uz, 1.0f));
+        I->vel, I->vel64, I->n, make_float4(ux, uy, uz, 1.0f));
     good = good && ok(grid, cudaGetLastError());
     good = good && ok(grid, cudaMemsetAsync(I->guard, 0, sizeof(unsigned long long), I->stream));
     good = good && sync(grid);
@@ -433,8 +452,8 @@ int LBM_InitializeFromField(LBMGrid *grid, const float *rho, const float *u) {
                                             cudaMemcpyHostToDevice, I->stream));
     good = good && ok(grid, launch_init_field(*I, I->pop[0], I->pop[1], drho, du, I->stream));
     if (good) {
-        k_vel_from_field<<<(unsigned)((I->n + 255) / 256), 256, 0, I->stream>>>(I->vel, I->n, drho,
-                                                                                 du);
+        k_vel_from_field<<<(unsigned)((I->n + 255) / 256), 256, 0, I->stream>>>(
+            I->vel, I->vel64, I->n, drho, du);
         good = ok(grid, cudaGetLastError());
     }
     good = good && ok(grid, cudaMemsetAsync(I->guard, 0, sizeof(unsigned long long), I->stream));
@@ -554,7 +573,7 @@ int LBM_ComputeDragForceF64(LBMGrid *grid, double *out6, long long *raw7) {
     const void *fexp = I->fbuf >= 0 ? I->pop[I->fbuf] : nullptr;
     const float4 *vel = I->vel_valid ? I->vel : nullptr;
     bool good = ok(grid, launch_force(*I, I->pop[I->gbuf], fexp, I->stream_periodic, vel,
-                                      I->pop[I->vin], I->vin_kind, I->vin_periodic, I->vin_inlet,
+                                      I->vel64, I->pop[I->vin], I->vin_kind, I->vin_periodic, I->vin_inlet,
                                       I->force_i64, I->force_f64, I->stream));
     long long *h = I->host_pinned;
     good = good && ok(grid, cudaMemcpyAsync(h, I->force_i64, sizeof(long long) * 7,
@@ -805,9 +824,11 @@ LBMParticles *LBM_ParticlesCreate(int n, unsigned int seed) {
     p->seed = seed;
     std::vector<LBMParticle> h((size_t)n);
     particles_seed_host(h.data(), n, seed);
-    if (cudaMalloc(&p->dev, sizeof(LBMParticle) * (size_t)n) != cudaSuccess ||
+    if (cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMalloc(&p->dev, sizeof(LBMParticle) * (size_t)n) != cudaSuccess ||
         cudaMemcpy(p->dev, h.data(), sizeof(LBMParticle) * (size_t)n, cudaMemcpyHostToDevice) !=
             cudaSuccess) {
+        if (p->done) cudaEventDestroy(p->done);
         cudaFree(p->dev);
         delete p;
         return nullptr;
@@ -817,7 +838,10 @@ LBMParticles *LBM_ParticlesCreate(int n, unsigned int seed) {
 
 void LBM_ParticlesFree(LBMParticles *p) {
     if (!p) return;
-    if (p->last) cudaStreamSynchronize(p->last);
+    if (p->done) {
+        cudaEventSynchronize(p->done);
+        cudaEventDestroy(p->done);
+    }
     cudaFree(p->dev);
     delete p;
 }
@@ -826,16 +850,15 @@ int LBM_ParticlesStep(LBMParticles *p, LBMGrid *grid, float dt) {
     GridImpl *I = IMPL(grid);
     if (!p || !I) return 0;
     if (!ensure_vel(grid)) return 0;
-    p->last = I->stream;
-    return ok(grid, launch_particles(p->dev, p->n, I->vel, I->nx, I->ny, I->nz, dt, p->seed,
-                                     I->stream))
-               ? 1
-               : 0;
+    if (!ok(grid, launch_particles(p->dev, p->n, I->vel, I->nx, I->ny, I->nz, dt, p->seed,
+                                   I->stream)))
+        return 0;
+    return ok(grid, cudaEventRecord(p->done, I->stream)) ? 1 : 0;
 }
 
 int LBM_ParticlesCopy(LBMParticles *p, LBMParticle *host) {
     if (!p || !host) return 0;
-    if (p->last && cudaStreamSynchronize(p->last) != cudaSuccess) return 0;
+    if (cudaEventSynchronize(p->done) != cudaSuccess) return 0;
     return cudaMemcpy(host, p->dev, sizeof(LBMParticle) * (size_t)p->n, cudaMemcpyDeviceToHost) ==
                    cudaSuccess
                ? 1
@@ -844,7 +867,7 @@ int LBM_ParticlesCopy(LBMParticles *p, LBMParticle *host) {
 
 int LBM_ParticlesLoad(LBMParticles *p, const LBMParticle *host) {
     if (!p || !host) return 0;
-    if (p->last && cudaStreamSynchronize(p->last) != cudaSuccess) return 0;
+    if (cudaEventSynchronize(p->done) != cudaSuccess) return 0;
     return cudaMemcpy(p->dev, host, sizeof(LBMParticle) * (size_t)p->n, cudaMemcpyHostToDevice) ==
                    cudaSuccess
                ? 1

@@ -57,17 +57,35 @@ enum : uint8_t {
 // Population storage formats.  R is the collision arithmetic type.
 // FP16/BF16 keep the deviation f_i - w_i (w_i in FP32).
 // ---------------------------------------------------------------------
+// load2/store2 move the populations of two neighbouring cells (p must be
+// aligned to two elements).
 struct StoreF32 {
     using T = float;
     using R = float;
     static __device__ __forceinline__ R load(const T *p, int) { return __ldg(p); }
     static __device__ __forceinline__ void store(T *p, R v, int) { *p = v; }
+    static __device__ __forceinline__ void load2(const T *p, int, R &a, R &b) {
+        const float2 v = __ldg(reinterpret_cast<const float2 *>(p));
+        a = v.x;
+        b = v.y;
+    }
+    static __device__ __forceinline__ void store2(T *p, R a, R b, int) {
+        *reinterpret_cast<float2 *>(p) = make_float2(a, b);
+    }
 };
 struct StoreF64 {
     using T = double;
     using R = double;
     static __device__ __forceinline__ R load(const T *p, int) { return __ldg(p); }
     static __device__ __forceinline__ void store(T *p, R v, int) { *p = v; }
+    static __device__ __forceinline__ void load2(const T *p, int, R &a, R &b) {
+        const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+        a = v.x;
+        b = v.y;
+    }
+    static __device__ __forceinline__ void store2(T *p, R a, R b, int) {
+        *reinterpret_cast<double2 *>(p) = make_double2(a, b);
+    }
 };
 struct StoreF16 {
     using T = __half;
@@ -78,6 +96,15 @@ struct StoreF16 {
     static __device__ __forceinline__ void store(T *p, R v, int i) {
         *p = __float2half_rn(v - wgt<float>(i));
     }
+    static __device__ __forceinline__ void load2(const T *p, int i, R &a, R &b) {
+        const __half2 v = __ldg(reinterpret_cast<const __half2 *>(p));
+        a = __low2float(v) + wgt<float>(i);
+        b = __high2float(v) + wgt<float>(i);
+    }
+    static __device__ __forceinline__ void store2(T *p, R a, R b, int i) {
+        *reinterpret_cast<__half2 *>(p) =
+            __halves2half2(__float2half_rn(a - wgt<float>(i)), __float2half_rn(b - wgt<float>(i)));
+    }
 };
 struct StoreBF16 {
     using T = __nv_bfloat16;
@@ -87,6 +114,15 @@ struct StoreBF16 {
     }
     static __device__ __forceinline__ void store(T *p, R v, int i) {
         *p = __float2bfloat16_rn(v - wgt<float>(i));
+    }
+    static __device__ __forceinline__ void load2(const T *p, int i, R &a, R &b) {
+        const __nv_bfloat162 v = __ldg(reinterpret_cast<const __nv_bfloat162 *>(p));
+        a = __low2float(v) + wgt<float>(i);
+        b = __high2float(v) + wgt<float>(i);
+    }
+    static __device__ __forceinline__ void store2(T *p, R a, R b, int i) {
+        *reinterpret_cast<__nv_bfloat162 *>(p) = __halves2bfloat162(
+            __float2bfloat16_rn(a - wgt<float>(i)), __float2bfloat16_rn(b - wgt<float>(i)));
     }
 };
 
@@ -109,6 +145,38 @@ template <> __device__ __forceinline__ double dsqrt<double>(double v) { return _
 template <typename R> __device__ __forceinline__ R ddiv(R a, R b);
 template <> __device__ __forceinline__ float ddiv<float>(float a, float b) { return __fdiv_rn(a, b); }
 template <> __device__ __forceinline__ double ddiv<double>(double a, double b) { return __ddiv_rn(a, b); }
+
+// Correctly rounded division by a constant y, given zh = RN(1/y):
+//   q1 = RN(x*zh); r = fma(-q1, y, x) (exact); q = fma(r, zh, q1)
+// (P. Markstein, IBM J. Res. Dev. 34(1), 1990).  For every divisor it is
+// used with, the sequence was checked against IEEE x / y on all 2^32
+// single-precision inputs (tests/native/cdiv_check.c): it agrees whenever
+// x == 0 or 2^-100 <= |x| <= 2^100.  Outside that range its result still
+// has magnitude below 2^-93 for |x| < 2^-100 (q1, r and q are all bounded
+// by a few |x|); the callers below only use it where such a value is
+// absorbed exactly as the IEEE quotient would be.  Double precision always
+// divides with the IEEE operation.
+template <typename R> __device__ __forceinline__ R cdiv(R x, R y, R zh);
+template <>
+__device__ __forceinline__ float cdiv<float>(float x, float y, float zh) {
+    const float q1 = __fmul_rn(x, zh);
+    const float r = __fmaf_rn(-q1, y, x);
+    return __fmaf_rn(r, zh, q1);
+}
+template <>
+__device__ __forceinline__ double cdiv<double>(double x, double y, double) {
+    return __ddiv_rn(x, y);
+}
+
+// a*b + c with one rounding.  Used only where a is +-2, +-4 or +-8, so the
+// product is exact and the result equals the separately rounded a*b + c.
+template <typename R> __device__ __forceinline__ R fmx(R a, R b, R c);
+template <> __device__ __forceinline__ float fmx<float>(float a, float b, float c) {
+    return __fmaf_rn(a, b, c);
+}
+template <> __device__ __forceinline__ double fmx<double>(double a, double b, double c) {
+    return __fma_rn(a, b, c);
+}
 
 // Zou-He boundaries (lbm_collide.comp:336-408); rewrite f in place.
 template <typename R>
@@ -142,29 +210,35 @@ __device__ __forceinline__ void zou_he_outlet(R (&f)[19]) {
     f[12] = f13 - (R(1) / R(6)) * rho_out * ux;
 }
 
+// length(u) > 0.40 of the guard.  sqrt is correctly rounded and monotone,
+// so in single precision RN(sqrt(u2)) > 0.4f exactly when u2 > 0x3e23d70b
+// (0.16000001f), the largest float whose rounded square root is 0.4f
+// (checked over every float in tests/test_const_division.py).
+__device__ __forceinline__ bool speed_exceeds(float u2) {
+    return u2 > __uint_as_float(0x3e23d70bu);
+}
+__device__ __forceinline__ bool speed_exceeds(double u2) { return __dsqrt_rn(u2) > 0.40; }
+
 // Macroscopic moments (:411-424) and the stability guard test (:429-430).
 // Returns true when the cell must be reset to feq(1, 0).
 template <typename R>
 __device__ __forceinline__ bool moments(const R (&f)[19], R &rho, R &ux, R &uy, R &uz) {
-    rho = R(0);
-    ux = R(0);
-    uy = R(0);
-    uz = R(0);
-#pragma unroll
-    for (int i = 0; i < 19; i++) {
-        R fi = f[i];
-        rho += fi;
-        ux += R(cx(i)) * fi;
-        uy += R(cy(i)) * fi;
-        uz += R(cz(i)) * fi;
-    }
+    // The shader accumulates rho += f_i and u += e_i f_i over i = 0..18.  The
+    // e-components are 0 or +-1, so u is the signed sum of the f_i with a
+    // nonzero component, in index order (a 0 * f_i term only adds a signed
+    // zero and cannot change a value).
+    rho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8] + f[9] + f[10] + f[11] +
+          f[12] + f[13] + f[14] + f[15] + f[16] + f[17] + f[18];
+    ux = f[1] - f[2] + f[7] - f[8] + f[9] - f[10] + f[11] - f[12] + f[13] - f[14];
+    uy = f[3] - f[4] + f[7] + f[8] - f[9] - f[10] + f[15] - f[16] + f[17] - f[18];
+    uz = f[5] - f[6] + f[11] + f[12] - f[13] - f[14] + f[15] + f[16] - f[17] - f[18];
     if (rho > R(0.0001)) {
         ux = ddiv<R>(ux, rho);
         uy = ddiv<R>(uy, rho);
         uz = ddiv<R>(uz, rho);
     }
-    R u_mag = dsqrt<R>(ux * ux + uy * uy + uz * uz);
-    return rho < R(0.3) || rho > R(2.0) || u_mag > R(0.40) || isinf(rho) || isnan(rho);
+    return rho < R(0.3) || rho > R(2.0) || speed_exceeds(ux * ux + uy * uy + uz * uz) ||
+           isinf(rho) || isnan(rho);
 }
 
 // Boundary/solid preprocessing shared by the step and the velocity
@@ -195,29 +269,31 @@ __device__ __forceinline__ int prepare_cell(R (&f)[19], int solid, int x, int nx
 // MRT transforms (lbm_collide.comp:110-181, :185-311)
 template <typename R>
 __device__ __forceinline__ void mrt_forward(const R (&fi)[19], R (&m)[19]) {
+    // Terms of the form (2^k) * s + t use one fused operation: the product
+    // by a power of two is exact, so the single rounding equals the
+    // shader's two.
     R sf = fi[1] + fi[2] + fi[3] + fi[4] + fi[5] + fi[6];
-    R se = fi[7] + fi[8] + fi[9] + fi[10] + fi[11] + fi[12] + fi[13] + fi[14] +
-           fi[15] + fi[16] + fi[17] + fi[18];
+    R se = fi[7] + fi[8] + fi[9] + fi[10] + fi[11] + fi[12] + fi[13] + fi[14] + fi[15] + fi[16] +
+           fi[17] + fi[18];
     m[0] = fi[0] + sf + se;
-    m[1] = R(-30) * fi[0] - R(11) * sf + R(8) * se;
-    m[2] = R(12) * fi[0] - R(4) * sf + se;
-    m[3] = fi[1] - fi[2] + fi[7] - fi[8] + fi[9] - fi[10] + fi[11] - fi[12] + fi[13] - fi[14];
-    m[4] = R(-4) * (fi[1] - fi[2]) + fi[7] - fi[8] + fi[9] - fi[10] + fi[11] - fi[12] +
-           fi[13] - fi[14];
-    m[5] = fi[3] - fi[4] + fi[7] + fi[8] - fi[9] - fi[10] + fi[15] - fi[16] + fi[17] - fi[18];
-    m[6] = R(-4) * (fi[3] - fi[4]) + fi[7] + fi[8] - fi[9] - fi[10] + fi[15] - fi[16] +
-           fi[17] - fi[18];
-    m[7] = fi[5] - fi[6] + fi[11] + fi[12] - fi[13] - fi[14] + fi[15] + fi[16] - fi[17] - fi[18];
-    m[8] = R(-4) * (fi[5] - fi[6]) + fi[11] + fi[12] - fi[13] - fi[14] + fi[15] + fi[16] -
-           fi[17] - fi[18];
-    R sXY = fi[7] + fi[8] + fi[9] + fi[10];
-    R sXZ = fi[11] + fi[12] + fi[13] + fi[14];
-    R sYZ = fi[15] + fi[16] + fi[17] + fi[18];
-    m[9] = R(2) * (fi[1] + fi[2]) - (fi[3] + fi[4]) - (fi[5] + fi[6]) + sXY + sXZ - R(2) * sYZ;
-    m[10] = R(-4) * (fi[1] + fi[2]) + R(2) * (fi[3] + fi[4]) + R(2) * (fi[5] + fi[6]) + sXY +
-            sXZ - R(2) * sYZ;
-    m[11] = (fi[3] + fi[4]) - (fi[5] + fi[6]) + sXY - sXZ;
-    m[12] = R(-2) * (fi[3] + fi[4]) + R(2) * (fi[5] + fi[6]) + sXY - sXZ;
+    m[1] = fmx<R>(R(8), se, R(-30) * fi[0] - R(11) * sf);
+    m[2] = fmx<R>(R(-4), sf, R(12) * fi[0]) + se;
+    const R d12 = fi[1] - fi[2], d34 = fi[3] - fi[4], d56 = fi[5] - fi[6];
+    m[3] = d12 + fi[7] - fi[8] + fi[9] - fi[10] + fi[11] - fi[12] + fi[13] - fi[14];
+    m[4] = fmx<R>(R(-4), d12, fi[7]) - fi[8] + fi[9] - fi[10] + fi[11] - fi[12] + fi[13] - fi[14];
+    m[5] = d34 + fi[7] + fi[8] - fi[9] - fi[10] + fi[15] - fi[16] + fi[17] - fi[18];
+    m[6] = fmx<R>(R(-4), d34, fi[7]) + fi[8] - fi[9] - fi[10] + fi[15] - fi[16] + fi[17] - fi[18];
+    m[7] = d56 + fi[11] + fi[12] - fi[13] - fi[14] + fi[15] + fi[16] - fi[17] - fi[18];
+    m[8] = fmx<R>(R(-4), d56, fi[11]) + fi[12] - fi[13] - fi[14] + fi[15] + fi[16] - fi[17] -
+           fi[18];
+    const R sXY = fi[7] + fi[8] + fi[9] + fi[10];
+    const R sXZ = fi[11] + fi[12] + fi[13] + fi[14];
+    const R sYZ = fi[15] + fi[16] + fi[17] + fi[18];
+    const R s12 = fi[1] + fi[2], s34 = fi[3] + fi[4], s56 = fi[5] + fi[6];
+    m[9] = fmx<R>(R(-2), sYZ, fmx<R>(R(2), s12, -s34) - s56 + sXY + sXZ);
+    m[10] = fmx<R>(R(-2), sYZ, fmx<R>(R(2), s56, fmx<R>(R(2), s34, R(-4) * s12)) + sXY + sXZ);
+    m[11] = s34 - s56 + sXY - sXZ;
+    m[12] = fmx<R>(R(2), s56, R(-2) * s34) + sXY - sXZ;
     m[13] = fi[7] - fi[8] - fi[9] + fi[10];
     m[14] = fi[15] - fi[16] - fi[17] + fi[18];
     m[15] = fi[11] - fi[12] - fi[13] + fi[14];
@@ -242,140 +318,189 @@ __device__ __forceinline__ void mrt_inverse(const R (&m)[19], R (&fi)[19]) {
     ms[10] = ddiv<R>(m[10], R(72));
     ms[11] = ddiv<R>(m[11], R(12));
     ms[12] = ddiv<R>(m[12], R(24));
-    ms[13] = m[13] * R(0.25);   // division by a power of two is exact
+    ms[13] = m[13] * R(0.25);  // division by a power of two is exact
     ms[14] = m[14] * R(0.25);
     ms[15] = m[15] * R(0.25);
     ms[16] = m[16] * R(0.125);
     ms[17] = m[17] * R(0.125);
     ms[18] = m[18] * R(0.125);
 
-    fi[0] = ms[0] - R(30) * ms[1] + R(12) * ms[2];
-    fi[1] = ms[0] - R(11) * ms[1] - R(4) * ms[2] + ms[3] - R(4) * ms[4] + R(2) * ms[9] -
-            R(4) * ms[10];
-    fi[2] = ms[0] - R(11) * ms[1] - R(4) * ms[2] - ms[3] + R(4) * ms[4] + R(2) * ms[9] -
-            R(4) * ms[10];
-    fi[3] = ms[0] - R(11) * ms[1] - R(4) * ms[2] + ms[5] - R(4) * ms[6] - ms[9] +
-            R(2) * ms[10] + ms[11] - R(2) * ms[12];
-    fi[4] = ms[0] - R(11) * ms[1] - R(4) * ms[2] - ms[5] + R(4) * ms[6] - ms[9] +
-            R(2) * ms[10] + ms[11] - R(2) * ms[12];
-    fi[5] = ms[0] - R(11) * ms[1] - R(4) * ms[2] + ms[7] - R(4) * ms[8] - ms[9] +
-            R(2) * ms[10] - ms[11] + R(2) * ms[12];
-    fi[6] = ms[0] - R(11) * ms[1] - R(4) * ms[2] - ms[7] + R(4) * ms[8] - ms[9] +
-            R(2) * ms[10] - ms[11] + R(2) * ms[12];
-    fi[7] = ms[0] + R(8) * ms[1] + ms[2] + ms[3] + ms[4] + ms[5] + ms[6] + ms[9] + ms[10] +
-            ms[11] + ms[12] + ms[13] + ms[16] - ms[17];
-    fi[8] = ms[0] + R(8) * ms[1] + ms[2] - ms[3] - ms[4] + ms[5] + ms[6] + ms[9] + ms[10] +
-            ms[11] + ms[12] - ms[13] - ms[16] - ms[17];
-    fi[9] = ms[0] + R(8) * ms[1] + ms[2] + ms[3] + ms[4] - ms[5] - ms[6] + ms[9] + ms[10] +
-            ms[11] + ms[12] - ms[13] + ms[16] + ms[17];
-    fi[10] = ms[0] + R(8) * ms[1] + ms[2] - ms[3] - ms[4] - ms[5] - ms[6] + ms[9] + ms[10] +
-             ms[11] + ms[12] + ms[13] - ms[16] + ms[17];
-    fi[11] = ms[0] + R(8) * ms[1] + ms[2] + ms[3] + ms[4] + ms[7] + ms[8] + ms[9] + ms[10] -
-             ms[11] - ms[12] + ms[15] - ms[16] + ms[18];
-    fi[12] = ms[0] + R(8) * ms[1] + ms[2] - ms[3] - ms[4] + ms[7] + ms[8] + ms[9] + ms[10] -
-             ms[11] - ms[12] - ms[15] + ms[16] + ms[18];
-    fi[13] = ms[0] + R(8) * ms[1] + ms[2] + ms[3] + ms[4] - ms[7] - ms[8] + ms[9] + ms[10] -
-             ms[11] - ms[12] - ms[15] - ms[16] - ms[18];
-    fi[14] = ms[0] + R(8) * ms[1] + ms[2] - ms[3] - ms[4] - ms[7] - ms[8] + ms[9] + ms[10] -
-             ms[11] - ms[12] + ms[15] + ms[16] - ms[18];
-    fi[15] = ms[0] + R(8) * ms[1] + ms[2] + ms[5] + ms[6] + ms[7] + ms[8] - R(2) * ms[9] -
-             R(2) * ms[10] + ms[14] + ms[17] - ms[18];
-    fi[16] = ms[0] + R(8) * ms[1] + ms[2] - ms[5] - ms[6] + ms[7] + ms[8] - R(2) * ms[9] -
-             R(2) * ms[10] - ms[14] - ms[17] - ms[18];
-    fi[17] = ms[0] + R(8) * ms[1] + ms[2] + ms[5] + ms[6] - ms[7] - ms[8] - R(2) * ms[9] -
-             R(2) * ms[10] - ms[14] + ms[17] + ms[18];
-    fi[18] = ms[0] + R(8) * ms[1] + ms[2] - ms[5] - ms[6] - ms[7] - ms[8] - R(2) * ms[9] -
-             R(2) * ms[10] + ms[14] - ms[17] + ms[18];
+    // lbm_collide.comp:210-310, left to right; products by 2, 4, 8 fused
+    fi[0] = (ms[0] - R(30) * ms[1]) + R(12) * ms[2];
+    const R a0 = fmx<R>(R(-4), ms[2], ms[0] - R(11) * ms[1]);  // ms0 - 11ms1 - 4ms2
+    fi[1] = fmx<R>(R(-4), ms[10], fmx<R>(R(2), ms[9], fmx<R>(R(-4), ms[4], a0 + ms[3])));
+    fi[2] = fmx<R>(R(-4), ms[10], fmx<R>(R(2), ms[9], fmx<R>(R(4), ms[4], a0 - ms[3])));
+    fi[3] = fmx<R>(R(-2), ms[12],
+                   fmx<R>(R(2), ms[10], fmx<R>(R(-4), ms[6], a0 + ms[5]) - ms[9]) + ms[11]);
+    fi[4] = fmx<R>(R(-2), ms[12],
+                   fmx<R>(R(2), ms[10], fmx<R>(R(4), ms[6], a0 - ms[5]) - ms[9]) + ms[11]);
+    fi[5] = fmx<R>(R(2), ms[12],
+                   fmx<R>(R(2), ms[10], fmx<R>(R(-4), ms[8], a0 + ms[7]) - ms[9]) - ms[11]);
+    fi[6] = fmx<R>(R(2), ms[12],
+                   fmx<R>(R(2), ms[10], fmx<R>(R(4), ms[8], a0 - ms[7]) - ms[9]) - ms[11]);
+    const R b0 = fmx<R>(R(8), ms[1], ms[0]) + ms[2];  // ms0 + 8ms1 + ms2
+    fi[7] = b0 + ms[3] + ms[4] + ms[5] + ms[6] + ms[9] + ms[10] + ms[11] + ms[12] + ms[13] + ms[16] -
+            ms[17];
+    fi[8] = b0 - ms[3] - ms[4] + ms[5] + ms[6] + ms[9] + ms[10] + ms[11] + ms[12] - ms[13] - ms[16] -
+            ms[17];
+    fi[9] = b0 + ms[3] + ms[4] - ms[5] - ms[6] + ms[9] + ms[10] + ms[11] + ms[12] - ms[13] + ms[16] +
+            ms[17];
+    fi[10] = b0 - ms[3] - ms[4] - ms[5] - ms[6] + ms[9] + ms[10] + ms[11] + ms[12] + ms[13] -
+             ms[16] + ms[17];
+    fi[11] = b0 + ms[3] + ms[4] + ms[7] + ms[8] + ms[9] + ms[10] - ms[11] - ms[12] + ms[15] -
+             ms[16] + ms[18];
+    fi[12] = b0 - ms[3] - ms[4] + ms[7] + ms[8] + ms[9] + ms[10] - ms[11] - ms[12] - ms[15] +
+             ms[16] + ms[18];
+    fi[13] = b0 + ms[3] + ms[4] - ms[7] - ms[8] + ms[9] + ms[10] - ms[11] - ms[12] - ms[15] -
+             ms[16] - ms[18];
+    fi[14] = b0 - ms[3] - ms[4] - ms[7] - ms[8] + ms[9] + ms[10] - ms[11] - ms[12] + ms[15] +
+             ms[16] - ms[18];
+    fi[15] = fmx<R>(R(-2), ms[10], fmx<R>(R(-2), ms[9], b0 + ms[5] + ms[6] + ms[7] + ms[8])) +
+             ms[14] + ms[17] - ms[18];
+    fi[16] = fmx<R>(R(-2), ms[10], fmx<R>(R(-2), ms[9], b0 - ms[5] - ms[6] + ms[7] + ms[8])) -
+             ms[14] - ms[17] - ms[18];
+    fi[17] = fmx<R>(R(-2), ms[10], fmx<R>(R(-2), ms[9], b0 + ms[5] + ms[6] - ms[7] - ms[8])) -
+             ms[14] + ms[17] + ms[18];
+    fi[18] = fmx<R>(R(-2), ms[10], fmx<R>(R(-2), ms[9], b0 - ms[5] - ms[6] - ms[7] - ms[8])) +
+             ms[14] - ms[17] + ms[18];
 }
 
-// Collision operators.  OP: 0 BGK, 1 regularized, 2 MRT.  `omega_tau`
-// is 1/tau precomputed on the host (the same IEEE quotient) and used when
-// SMAG is off.
+// Equilibria of the 19 directions (lbm_collide.comp:94-101):
+//   feq_i = (w_i rho) * (((1 + eu_i/cs2) + eu_i^2/(2 cs2^2)) - u^2/(2 cs2))
+// with eu_i evaluated exactly as the shader's (e_x ux + e_y uy) + e_z uz.
+// Opposite directions have eu_j = -eu_i, and rounding is sign-symmetric,
+// so each pair shares its two quotients.  The quotients by the constants
+// use cdiv: when |eu| >= 2^-50 (and u^2 >= 2^-100) every operand is in the
+// verified range; when |eu| < 2^-50, eu/cs2 and eu^2/(2cs2^2) are below
+// 2^-90 under either division, and 1 + a, (1 + a) + b and s - cu round to
+// the same floats, so the result is the IEEE one in every case.
+template <typename R>
+__device__ __forceinline__ void equilibria(R rho, R ux, R uy, R uz, R (&fe)[19]) {
+    constexpr R cs2 = R(1) / R(3);
+    constexpr R c1 = R(2) * cs2;
+    constexpr R c2 = R(2) * cs2 * cs2;
+    const R u2 = ux * ux + uy * uy + uz * uz;
+    const R cu = cdiv<R>(u2, c1, R(1) / c1);
+    const R wr0 = wgt<R>(0) * rho, wr1 = wgt<R>(1) * rho, wr2 = wgt<R>(7) * rho;
+    fe[0] = wr0 * (R(1) - cu);
+    auto pair = [&](R e, R wr, R &fi, R &fj) {
+        const R a = cdiv<R>(e, cs2, R(1) / cs2);
+        const R b = cdiv<R>(e * e, c2, R(1) / c2);
+        fi = wr * (((R(1) + a) + b) - cu);
+        fj = wr * (((R(1) - a) + b) - cu);
+    };
+    pair(ux, wr1, fe[1], fe[2]);
+    pair(uy, wr1, fe[3], fe[4]);
+    pair(uz, wr1, fe[5], fe[6]);
+    pair(ux + uy, wr2, fe[7], fe[10]);
+    pair(uy - ux, wr2, fe[8], fe[9]);
+    pair(ux + uz, wr2, fe[11], fe[14]);
+    pair(uz - ux, wr2, fe[12], fe[13]);
+    pair(uy + uz, wr2, fe[15], fe[18]);
+    pair(uz - uy, wr2, fe[16], fe[17]);
+}
 
+// Non-equilibrium stress Pi_ab = sum_i e_ia e_ib (f_i - feq_i)
+// (lbm_collide.comp:455-470, identical to :500-515), nonzero terms in
+// index order.
+template <typename R>
+__device__ __forceinline__ void stress(const R (&f)[19], const R (&fe)[19], R &Pxx, R &Pyy,
+                                       R &Pzz, R &Pxy, R &Pxz, R &Pyz) {
+    R n[19];
+#pragma unroll
+    for (int i = 0; i < 19; i++) n[i] = f[i] - fe[i];
+    Pxx = n[1] + n[2] + n[7] + n[8] + n[9] + n[10] + n[11] + n[12] + n[13] + n[14];
+    Pyy = n[3] + n[4] + n[7] + n[8] + n[9] + n[10] + n[15] + n[16] + n[17] + n[18];
+    Pzz = n[5] + n[6] + n[11] + n[12] + n[13] + n[14] + n[15] + n[16] + n[17] + n[18];
+    Pxy = n[7] - n[8] - n[9] + n[10];
+    Pxz = n[11] - n[12] - n[13] + n[14];
+    Pyz = n[15] - n[16] - n[17] + n[18];
+}
+
+// Collision (lbm_collide.comp:445-625).  OP: 0 BGK, 1 regularized, 2 MRT.
+// `omega_tau` is 1/tau computed on the host (the same IEEE quotient) and
+// used when SMAG is off; `smag18` is 18*Cs*Cs.
 template <typename R, int OP, bool SMAG>
-__device__ __forceinline__ void collide(const R (&f)[19], R (&fn)[19], R rho, R ux, R uy,
-                                        R uz, R tau, R omega_tau, R smagCs) {
+__device__ __forceinline__ void collide(const R (&f)[19], R (&fn)[19], R rho, R ux, R uy, R uz,
+                                        R tau, R omega_tau, R smag18) {
     R fe[19];
-    if (SMAG || OP != OP_MRT) {
-#pragma unroll
-        for (int i = 0; i < 19; i++) fe[i] = feq<R>(i, rho, ux, uy, uz);
-    }
+    if (SMAG || OP != OP_MRT) equilibria<R>(rho, ux, uy, uz, fe);
     R omega = omega_tau;
+    R Pxx, Pyy, Pzz, Pxy, Pxz, Pyz;
+    if (SMAG || OP == OP_REG) stress<R>(f, fe, Pxx, Pyy, Pzz, Pxy, Pxz, Pyz);
     if (SMAG) {
-        // :448-484
-        R Sxx = R(0), Syy = R(0), Szz = R(0), Sxy = R(0), Sxz = R(0), Syz = R(0);
-#pragma unroll
-        for (int i = 0; i < 19; i++) {
-            R f_neq = f[i] - fe[i];
-            R ex = R(cx(i)), ey = R(cy(i)), ez = R(cz(i));
-            Sxx += ex * ex * f_neq;
-            Syy += ey * ey * f_neq;
-            Szz += ez * ez * f_neq;
-            Sxy += ex * ey * f_neq;
-            Sxz += ex * ez * f_neq;
-            Syz += ey * ez * f_neq;
-        }
-        R Pi_norm = dsqrt<R>(Sxx * Sxx + Syy * Syy + Szz * Szz +
-                             R(2) * (Sxy * Sxy + Sxz * Sxz + Syz * Syz));
-        R Cs2 = smagCs * smagCs;
-        R tau_eff = R(0.5) * (tau + dsqrt<R>(tau * tau + ddiv<R>(R(18) * Cs2 * Pi_norm,
-                                                                  rho + R(1e-10))));
+        // :472-484
+        const R Pi_norm = dsqrt<R>(
+            fmx<R>(R(2), Pxy * Pxy + Pxz * Pxz + Pyz * Pyz, Pxx * Pxx + Pyy * Pyy + Pzz * Pzz));
+        const R tau_eff =
+            R(0.5) * (tau + dsqrt<R>(tau * tau + ddiv<R>(smag18 * Pi_norm, rho + R(1e-10))));
         omega = ddiv<R>(R(1), tau_eff);
     }
     if (OP == OP_REG) {
-        // :488-543
-        R Pxx = R(0), Pyy = R(0), Pzz = R(0), Pxy = R(0), Pxz = R(0), Pyz = R(0);
+        // :517-543: f_i = feq_i + (1 - omega) (w_i 4.5) Q_i:Pi, Q_i:Pi summed
+        // in the shader's order with the zero products dropped
+        constexpr R cs2 = R(1) / R(3);
+        constexpr R k1 = R(1) - cs2;  // e_a^2 - cs2 for e_a = +-1
+        constexpr R k0 = R(0) - cs2;  // e_a^2 - cs2 for e_a = 0
+        const R om = R(1) - omega;
+        const R Q0 = (k0 * Pxx + k0 * Pyy) + k0 * Pzz;
+        const R Qx = (k1 * Pxx + k0 * Pyy) + k0 * Pzz;
+        const R Qy = (k0 * Pxx + k1 * Pyy) + k0 * Pzz;
+        const R Qz = (k0 * Pxx + k0 * Pyy) + k1 * Pzz;
+        const R Txy = (k1 * Pxx + k1 * Pyy) + k0 * Pzz;
+        const R Txz = (k1 * Pxx + k0 * Pyy) + k1 * Pzz;
+        const R Tyz = (k0 * Pxx + k1 * Pyy) + k1 * Pzz;
+        R Q[19];
+        Q[0] = Q0;
+        Q[1] = Q[2] = Qx;
+        Q[3] = Q[4] = Qy;
+        Q[5] = Q[6] = Qz;
+        Q[7] = Q[10] = fmx<R>(R(2), Pxy, Txy);
+        Q[8] = Q[9] = fmx<R>(R(-2), Pxy, Txy);
+        Q[11] = Q[14] = fmx<R>(R(2), Pxz, Txz);
+        Q[12] = Q[13] = fmx<R>(R(-2), Pxz, Txz);
+        Q[15] = Q[18] = fmx<R>(R(2), Pyz, Tyz);
+        Q[16] = Q[17] = fmx<R>(R(-2), Pyz, Tyz);
 #pragma unroll
-        for (int i = 0; i < 19; i++) {
-            R f_neq = f[i] - fe[i];
-            R ex = R(cx(i)), ey = R(cy(i)), ez = R(cz(i));
-            Pxx += ex * ex * f_neq;
-            Pyy += ey * ey * f_neq;
-            Pzz += ez * ez * f_neq;
-            Pxy += ex * ey * f_neq;
-            Pxz += ex * ez * f_neq;
-            Pyz += ey * ez * f_neq;
-        }
-        const R inv_2cs4 = R(4.5);
-        const R cs2 = R(1) / R(3);
-#pragma unroll
-        for (int i = 0; i < 19; i++) {
-            R ex = R(cx(i)), ey = R(cy(i)), ez = R(cz(i));
-            R QP = (ex * ex - cs2) * Pxx + (ey * ey - cs2) * Pyy + (ez * ez - cs2) * Pzz +
-                   R(2) * ex * ey * Pxy + R(2) * ex * ez * Pxz + R(2) * ey * ez * Pyz;
-            R f_neq_reg = wgt<R>(i) * inv_2cs4 * QP;
-            fn[i] = fe[i] + (R(1) - omega) * f_neq_reg;
-        }
+        for (int i = 0; i < 19; i++) fn[i] = fe[i] + om * ((wgt<R>(i) * R(4.5)) * Q[i]);
     } else if (OP == OP_MRT) {
-        // :544-617
+        // :550-616
         R m[19], meq[19];
         mrt_forward<R>(f, m);
-        R u2 = ux * ux + uy * uy + uz * uz;
-        meq[0] = rho;
+        const R uyy = uy * uy, uzz = uz * uz;
+        const R u2 = ux * ux + uyy + uzz;
+        const R pxx = R(2) * ux * ux - uyy - uzz;  // (2 ux) ux - uy^2 - uz^2
+        const R pww = uyy - uzz;
         meq[1] = R(-11) * rho + R(19) * rho * u2;
         meq[2] = R(3) * rho - R(5.5) * rho * u2;
-        meq[3] = rho * ux;
         meq[4] = R(-2) / R(3) * rho * ux;
-        meq[5] = rho * uy;
         meq[6] = R(-2) / R(3) * rho * uy;
-        meq[7] = rho * uz;
         meq[8] = R(-2) / R(3) * rho * uz;
-        meq[9] = rho * (R(2) * ux * ux - uy * uy - uz * uz);
-        meq[10] = R(-0.5) * rho * (R(2) * ux * ux - uy * uy - uz * uz);
-        meq[11] = rho * (uy * uy - uz * uz);
-        meq[12] = R(-0.5) * rho * (uy * uy - uz * uz);
+        meq[9] = rho * pxx;
+        meq[10] = R(-0.5) * rho * pxx;
+        meq[11] = rho * pww;
+        meq[12] = R(-0.5) * rho * pww;
         meq[13] = rho * ux * uy;
         meq[14] = rho * uy * uz;
         meq[15] = rho * ux * uz;
-        meq[16] = R(0);
-        meq[17] = R(0);
-        meq[18] = R(0);
         const R s_nu = omega;
-        const R s[19] = {R(0),    R(1.19), R(1.4), R(0),  R(1.2), R(0),    R(1.2),
-                         R(0),    R(1.2),  s_nu,   R(1.4), s_nu,  R(1.4),  s_nu,
-                         s_nu,    s_nu,    R(1.98), R(1.98), R(1.98)};
-#pragma unroll
-        for (int k = 0; k < 19; k++) m[k] = m[k] - s[k] * (m[k] - meq[k]);
+        // relaxation m - s (m - meq); the conserved moments 0, 3, 5, 7 have
+        // s = 0 and keep their value; meq of the ghost modes 16-18 is 0
+        m[1] = m[1] - R(1.19) * (m[1] - meq[1]);
+        m[2] = m[2] - R(1.4) * (m[2] - meq[2]);
+        m[4] = m[4] - R(1.2) * (m[4] - meq[4]);
+        m[6] = m[6] - R(1.2) * (m[6] - meq[6]);
+        m[8] = m[8] - R(1.2) * (m[8] - meq[8]);
+        m[9] = m[9] - s_nu * (m[9] - meq[9]);
+        m[10] = m[10] - R(1.4) * (m[10] - meq[10]);
+        m[11] = m[11] - s_nu * (m[11] - meq[11]);
+        m[12] = m[12] - R(1.4) * (m[12] - meq[12]);
+        m[13] = m[13] - s_nu * (m[13] - meq[13]);
+        m[14] = m[14] - s_nu * (m[14] - meq[14]);
+        m[15] = m[15] - s_nu * (m[15] - meq[15]);
+        m[16] = m[16] - R(1.98) * m[16];
+        m[17] = m[17] - R(1.98) * m[17];
+        m[18] = m[18] - R(1.98) * m[18];
         mrt_inverse<R>(m, fn);
     } else {
         // :618-625

@@ -47,12 +47,13 @@ cudaError_t launch_stream_only(const GridImpl &g, const void *src, void *dst, in
 }
 
 cudaError_t launch_velocity(const GridImpl &g, const void *src, int kind, int periodic,
-                            float inX, float inY, float inZ, float4 *vel, cudaStream_t s) {
+                            float inX, float inY, float inZ, float4 *vel, double4 *vel64,
+                            cudaStream_t s) {
     StepArgs a = stream_args(g, src, nullptr, periodic);
     a.inX = inX;
     a.inY = inY;
     a.inZ = inZ;
-    LBM_DISPATCH(g.storage, velocity(g, a, kind, vel, s));
+    LBM_DISPATCH(g.storage, velocity(g, a, kind, vel, vel64, s));
 }
 
 cudaError_t launch_init_uniform(const GridImpl &g, void *a, void *b, float ux, float uy,

@@ -21,6 +21,7 @@ struct ForceArgs {
     const int32_t *bcell;     // boundary cells
     const void *fexp;         // explicit post-stream f, or null
     const float4 *vel;        // valid velocity field, or null
+    const double4 *vel64;     // its FP64 copy (FP64 grids), or null
     StepArgs vin;             // input of the last step when vel is null
     int vin_kind;
     long long *i64;
@@ -55,7 +56,13 @@ __global__ void __launch_bounds__(128) k_force(const ForceArgs a, int nb) {
             const int z = (int)(r / ny);
             // velocity and density of the last collide
             R rho, ux, uy, uz;
-            if (a.vel) {
+            if (a.vel64) {
+                const double4 v = a.vel64[cell];
+                ux = R(v.x);
+                uy = R(v.y);
+                uz = R(v.z);
+                rho = R(v.w);
+            } else if (a.vel) {
                 const float4 v = a.vel[cell];
                 ux = R(v.x);
                 uy = R(v.y);
@@ -181,7 +188,8 @@ cudaError_t force_launch(const ForceArgs &a, int nb, cudaStream_t s) {
 }  // namespace
 
 cudaError_t launch_force(const GridImpl &g, const void *gsrc, const void *f_explicit,
-                         int periodic, const float4 *vel_or_null, const void *vin_src,
+                         int periodic, const float4 *vel_or_null, const double4 *vel64_or_null,
+                         const void *vin_src,
                          int vin_kind, int vin_periodic, const float vin_inlet[3],
                          long long *i64, double *f64, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(i64, 0, sizeof(long long) * 7, s);
@@ -203,6 +211,7 @@ cudaError_t launch_force(const GridImpl &g, const void *gsrc, const void *f_expl
     a.st.periodic = periodic;
     a.fexp = f_explicit;
     a.vel = vel_or_null;
+    a.vel64 = vel_or_null ? vel64_or_null : nullptr;
     a.vin = a.st;
     a.vin.src = vin_src;
     a.vin.periodic = vin_periodic;

@@ -48,6 +48,7 @@ struct GridImpl {
 
     void *pop[2] = {nullptr, nullptr};  // SoA planes pop[i * n + cell]
     float4 *vel = nullptr;
+    double4 *vel64 = nullptr;           // FP64 grids: full-precision copy of vel
     int32_t *solid = nullptr;
     uint8_t *flags = nullptr;
     int32_t *slot = nullptr;            // boundary-cell index or -1
@@ -70,8 +71,9 @@ struct GridImpl {
     int vin_periodic = 0;     // periodic flag of the stream feeding vin (post-collision kind)
     float vin_inlet[3] = {0, 0, 0};
 
-    // launch configuration of the step kernel (autotuned)
-    int bx = 128, by = 1;
+    // launch configuration of the step kernel: block shape and cells per
+    // thread along x
+    int bx = 128, by = 1, cpt = 1, minb = 1;
 
     // CUDA graphs for LBM_StepN, one per starting buffer parity (gbuf)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -89,7 +91,8 @@ struct StepArgs {
     int nx, ny, nz;
     long long n;
     int periodic;      // periodic flag of the stream part
-    float tau, omega, smagCs;
+    float tau, omega, smag18;   // omega = 1/tau, smag18 = 18*Cs*Cs (FP32 arithmetic)
+    double omega_d, smag18_d;   // the same in FP64 arithmetic (FP64 storage)
     float inX, inY, inZ;
     unsigned long long *guard;
 };
@@ -100,7 +103,8 @@ cudaError_t launch_step(const GridImpl &g, const StepArgs &a, bool fused, int op
 cudaError_t launch_stream_only(const GridImpl &g, const void *src, void *dst, int periodic,
                                cudaStream_t s);
 cudaError_t launch_velocity(const GridImpl &g, const void *src, int kind, int periodic,
-                            float inX, float inY, float inZ, float4 *vel, cudaStream_t s);
+                            float inX, float inY, float inZ, float4 *vel, double4 *vel64,
+                            cudaStream_t s);
 cudaError_t launch_init_uniform(const GridImpl &g, void *a, void *b, float ux, float uy,
                                 float uz, cudaStream_t s);
 cudaError_t launch_init_field(const GridImpl &g, void *a, void *b, const float *rho,
@@ -127,7 +131,8 @@ void geo_free_links(LinkList &l);
 
 // lbm_force.cu
 cudaError_t launch_force(const GridImpl &g, const void *gsrc, const void *f_explicit,
-                         int periodic, const float4 *vel_or_null, const void *vin_src,
+                         int periodic, const float4 *vel_or_null, const double4 *vel64_or_null,
+                         const void *vin_src,
                          int vin_kind, int vin_periodic, const float vin_inlet[3],
                          long long *i64, double *f64, cudaStream_t s);
 

@@ -21,15 +21,13 @@
 
 namespace lbm {
 
-// Pull-stream gather of the post-stream populations of one cell from the
-// post-collision field `src` (lbm_stream.comp:85-128).
-template <class S>
-__device__ __forceinline__ void gather_stream(const StepArgs &a, const typename S::T *__restrict__ src,
-                                              int x, int y, int z, long long cell, uint8_t flag,
-                                              typename S::R (&f)[19]) {
-    using R = typename S::R;
-    const long long n = a.n;
-    const int nx = a.nx, ny = a.ny, nz = a.nz;
+// Row offsets of the y/z neighbours of a cell after the reference's
+// wrap (periodic) or clamp rule (lbm_stream.comp:63-74).
+struct Rows {
+    long long y[3], z[3];  // index 0: coordinate - 1, 1: itself, 2: + 1
+};
+__device__ __forceinline__ Rows neighbour_rows(const StepArgs &a, int y, int z) {
+    const int ny = a.ny, nz = a.nz;
     int ym = y - 1, yp = y + 1, zm = z - 1, zp = z + 1;
     if (a.periodic == 1) {
         if (ym < 0) ym += ny;
@@ -42,90 +40,206 @@ __device__ __forceinline__ void gather_stream(const StepArgs &a, const typename 
         zm = zm < 0 ? 0 : zm;
         zp = zp > nz - 1 ? nz - 1 : zp;
     }
-    const long long plane = (long long)nx * ny;
-    const long long rowY[3] = {(long long)ym * nx, (long long)y * nx, (long long)yp * nx};
-    const long long rowZ[3] = {(long long)zm * plane, (long long)z * plane, (long long)zp * plane};
+    const long long nx = a.nx, plane = (long long)a.nx * a.ny;
+    Rows r;
+    r.y[0] = ym * nx;
+    r.y[1] = y * nx;
+    r.y[2] = yp * nx;
+    r.z[0] = zm * plane;
+    r.z[1] = z * plane;
+    r.z[2] = zp * plane;
+    return r;
+}
 
+// Plain pull of one cell anywhere in the grid (lbm_stream.comp:116-127):
+// source x - e_x, y/z wrapped or clamped, own value when the source x is
+// outside the grid.
+template <class S>
+__device__ __forceinline__ void gather_pull(const StepArgs &a, const typename S::T *__restrict__ src,
+                                            int x, const Rows &rw, long long cell,
+                                            typename S::R (&f)[19]) {
+    const long long n = a.n;
 #pragma unroll
     for (int i = 0; i < 19; i++) {
         const int sx = x - cx(i);
         const long long sidx =
-            (sx < 0 || sx >= nx) ? cell : rowY[1 - cy(i)] + rowZ[1 - cz(i)] + sx;
+            (sx < 0 || sx >= a.nx) ? cell : rw.y[1 - cy(i)] + rw.z[1 - cz(i)] + sx;
         f[i] = S::load(src + (long long)i * n + sidx, i);
     }
+}
 
-    if (flag & FLAG_BOUNDARY) {
-        const int b = a.slot[cell];
-        const uint32_t mask = a.bmask[b];
-        const int first = a.bfirst[b];
+// Pull of CPT consecutive cells (cell0 even when CPT == 2) whose neighbours
+// are all inside the grid: every direction reads at a warp-uniform offset
+// from the cell, and the directions with e_x == 0 read both cells with one
+// aligned pair load.
+template <class S, int CPT>
+__device__ __forceinline__ void gather_interior(const StepArgs &a,
+                                                const typename S::T *__restrict__ src,
+                                                long long cell0, typename S::R (&f0)[19],
+                                                typename S::R (&f1)[19]) {
+    const typename S::T *p = src + cell0;
+    const long long n = a.n, nx = a.nx, plane = (long long)a.nx * a.ny;
 #pragma unroll
-        for (int i = 0; i < 19; i++) {
-            const int io = opp(i);
-            if (mask & (1u << io)) {
-                const float q = a.lq[first + __popc(mask & ((1u << io) - 1u))];
-                const R fiopp = S::load(src + (long long)io * n + cell, io);
-                const R qq = R(q);
-                if (q >= 0.5f) {
-                    const R fi = S::load(src + (long long)i * n + cell, i);
-                    const R inv2q = ddiv<R>(R(1), R(2) * qq);
-                    f[i] = inv2q * fiopp + (R(1) - inv2q) * fi;
-                } else {
-                    const int fx = x + cx(i);
-                    R ff;
-                    if (fx >= 0 && fx < nx)
-                        ff = S::load(src + (long long)io * n + rowY[1 + cy(i)] +
-                                         rowZ[1 + cz(i)] + fx,
-                                     io);
-                    else
-                        ff = fiopp;
-                    const R twoq = R(2) * qq;
-                    f[i] = twoq * fiopp + (R(1) - twoq) * ff;
-                }
+    for (int i = 0; i < 19; i++) {
+        const long long off = (long long)i * n - cx(i) - cy(i) * nx - cz(i) * plane;
+        if (CPT == 2 && cx(i) == 0) {
+            S::load2(p + off, i, f0[i], f1[i]);
+        } else {
+            f0[i] = S::load(p + off, i);
+            if (CPT == 2) f1[i] = S::load(p + off + 1, i);
+        }
+    }
+}
+
+// Bouzidi interpolated bounce-back on the links of one boundary cell
+// (lbm_stream.comp:88-115): overwrites the pulled value of every direction
+// i whose opposite direction has a link with q >= 0.
+template <class S>
+__device__ __forceinline__ void bouzidi(const StepArgs &a, const typename S::T *__restrict__ src,
+                                        int x, const Rows &rw, long long cell,
+                                        typename S::R (&f)[19]) {
+    using R = typename S::R;
+    const long long n = a.n;
+    const int b = a.slot[cell];
+    const uint32_t mask = a.bmask[b];
+    const int first = a.bfirst[b];
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        const int io = opp(i);
+        if (mask & (1u << io)) {
+            const float q = a.lq[first + __popc(mask & ((1u << io) - 1u))];
+            const R fiopp = S::load(src + (long long)io * n + cell, io);
+            const R qq = R(q);
+            if (q >= 0.5f) {
+                const R fi = S::load(src + (long long)i * n + cell, i);
+                const R inv2q = ddiv<R>(R(1), R(2) * qq);
+                f[i] = inv2q * fiopp + (R(1) - inv2q) * fi;
+            } else {
+                const int fx = x + cx(i);
+                R ff;
+                if (fx >= 0 && fx < a.nx)
+                    ff = S::load(src + (long long)io * n + rw.y[1 + cy(i)] + rw.z[1 + cz(i)] + fx,
+                                 io);
+                else
+                    ff = fiopp;
+                const R twoq = R(2) * qq;
+                f[i] = twoq * fiopp + (R(1) - twoq) * ff;
             }
         }
     }
 }
 
-template <class S, int OP, bool SMAG, bool FUSED>
-__global__ void __launch_bounds__(256) k_step(const StepArgs a) {
-    using T = typename S::T;
+// Full pull-stream gather of one cell (plain pull + Bouzidi links).
+template <class S>
+__device__ __forceinline__ void gather_stream(const StepArgs &a, const typename S::T *__restrict__ src,
+                                              int x, int y, int z, long long cell, uint8_t flag,
+                                              typename S::R (&f)[19]) {
+    const Rows rw = neighbour_rows(a, y, z);
+    gather_pull<S>(a, src, x, rw, cell, f);
+    if (flag & FLAG_BOUNDARY) bouzidi<S>(a, src, x, rw, cell, f);
+}
+
+// Collision of one cell after the stream: solid rule, Zou-He, guard, then
+// the operator.
+template <class S, int OP, bool SMAG>
+__device__ __forceinline__ int collide_cell(const StepArgs &a, typename S::R (&f)[19],
+                                            typename S::R (&fn)[19], int x, uint8_t flag) {
     using R = typename S::R;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z;
-    if (x >= a.nx || y >= a.ny) return;
-    const long long n = a.n;
-    const long long cell = (long long)x + (long long)a.nx * ((long long)y + (long long)a.ny * z);
-    const uint8_t flag = a.flags[cell];
-    const T *__restrict__ src = static_cast<const T *>(a.src);
-    T *__restrict__ dst = static_cast<T *>(a.dst);
-
-    R f[19];
-    if (FUSED) {
-        gather_stream<S>(a, src, x, y, z, cell, flag, f);
-    } else {
-#pragma unroll
-        for (int i = 0; i < 19; i++) f[i] = S::load(src + (long long)i * n + cell, i);
-    }
-
     R rho, ux, uy, uz;
     const int kind = prepare_cell<R>(f, flag & FLAG_SOLID_MASK, x, a.nx, R(a.inX), R(a.inY),
                                      R(a.inZ), rho, ux, uy, uz);
-    R fn[19];
     if (kind == 1) {
 #pragma unroll
         for (int i = 0; i < 19; i++) fn[i] = f[opp(i)];
     } else if (kind == 2) {
 #pragma unroll
-        for (int i = 0; i < 19; i++) fn[i] = feq<R>(i, R(1), R(0), R(0), R(0));
+        for (int i = 0; i < 19; i++) fn[i] = wgt<R>(i);  // feq(1, 0): w_i * 1 * (((1+0)+0)-0)
     } else {
-        collide<R, OP, SMAG>(f, fn, rho, ux, uy, uz, R(a.tau), R(a.omega), R(a.smagCs));
+        const R omega = sizeof(R) == 8 ? R(a.omega_d) : R(a.omega);
+        const R smag18 = sizeof(R) == 8 ? R(a.smag18_d) : R(a.smag18);
+        collide<R, OP, SMAG>(f, fn, rho, ux, uy, uz, R(a.tau), omega, smag18);
     }
-    const unsigned reset = __ballot_sync(__activemask(), kind == 2);
-    if (reset && (threadIdx.x & 31) == (unsigned)(__ffs(reset) - 1))
-        atomicAdd(a.guard, (unsigned long long)__popc(reset));
+    return kind;
+}
+
+// The step.  CPT = cells per thread along x (1 or 2; 2 needs an even NX).
+template <class S, int OP, bool SMAG, bool FUSED, int CPT, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_step(const StepArgs a) {
+    using T = typename S::T;
+    using R = typename S::R;
+    const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * CPT;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x0 >= a.nx || y >= a.ny) return;
+    const long long n = a.n;
+    const long long cell0 =
+        (long long)x0 + (long long)a.nx * ((long long)y + (long long)a.ny * z);
+    const T *__restrict__ src = static_cast<const T *>(a.src);
+    T *__restrict__ dst = static_cast<T *>(a.dst);
+
+    uint8_t flag0, flag1 = 0;
+    if (CPT == 2) {
+        const uchar2 fl = *reinterpret_cast<const uchar2 *>(a.flags + cell0);
+        flag0 = fl.x;
+        flag1 = fl.y;
+    } else {
+        flag0 = a.flags[cell0];
+    }
+
+    R cur[19], nxt[19];
+    if (FUSED) {
+        const bool interior = x0 > 0 && x0 + CPT < a.nx && y > 0 && y + 1 < a.ny && z > 0 &&
+                              z + 1 < a.nz;
+        const Rows rw = neighbour_rows(a, y, z);
+        if (interior) {
+            gather_interior<S, CPT>(a, src, cell0, cur, nxt);
+        } else {
+            gather_pull<S>(a, src, x0, rw, cell0, cur);
+            if (CPT == 2) gather_pull<S>(a, src, x0 + 1, rw, cell0 + 1, nxt);
+        }
+        if (flag0 & FLAG_BOUNDARY) bouzidi<S>(a, src, x0, rw, cell0, cur);
+        if (CPT == 2 && (flag1 & FLAG_BOUNDARY)) bouzidi<S>(a, src, x0 + 1, rw, cell0 + 1, nxt);
+    } else {
 #pragma unroll
-    for (int i = 0; i < 19; i++) S::store(dst + (long long)i * n + cell, fn[i], i);
+        for (int i = 0; i < 19; i++) {
+            cur[i] = S::load(src + (long long)i * n + cell0, i);
+            if (CPT == 2) nxt[i] = S::load(src + (long long)i * n + cell0 + 1, i);
+        }
+    }
+
+    // One code instance of the collision for both cells; the second cell's
+    // populations rotate into `cur`, the first cell's results wait in `keep`.
+    R keep[19];
+    int resets = 0;
+#pragma unroll 1
+    for (int c = 0; c < CPT; c++) {
+        R fn[19];
+        const int kind = collide_cell<S, OP, SMAG>(a, cur, fn, x0 + c, c ? flag1 : flag0);
+        resets += kind == 2;
+        if (c == CPT - 1) {
+#pragma unroll
+            for (int i = 0; i < 19; i++) {
+                if (CPT == 2)
+                    S::store2(dst + (long long)i * n + cell0, keep[i], fn[i], i);
+                else
+                    S::store(dst + (long long)i * n + cell0, fn[i], i);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 19; i++) {
+                keep[i] = fn[i];
+                cur[i] = nxt[i];
+            }
+        }
+    }
+    const unsigned active = __activemask();
+    const unsigned any = __ballot_sync(active, resets > 0);
+    if (any) {
+        int v = resets;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(active, v, o);
+        if ((threadIdx.x & 31) == (unsigned)(__ffs(active) - 1) && v)
+            atomicAdd(a.guard, (unsigned long long)v);
+    }
 }
 
 // Stream only: materialise the post-stream populations f = Stream(g).
@@ -149,7 +263,8 @@ __global__ void __launch_bounds__(256) k_stream_only(const StepArgs a) {
 // Velocity/density of a step (lbm_collide.comp:322-443): the moments of the
 // step's input after the solid rule, Zou-He and the guard.
 template <class S>
-__global__ void __launch_bounds__(256) k_velocity(const StepArgs a, int kind_in, float4 *vel) {
+__global__ void __launch_bounds__(256) k_velocity(const StepArgs a, int kind_in, float4 *vel,
+                                                   double4 *vel64) {
     using T = typename S::T;
     using R = typename S::R;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -171,6 +286,7 @@ __global__ void __launch_bounds__(256) k_velocity(const StepArgs a, int kind_in,
     prepare_cell<R>(f, flag & FLAG_SOLID_MASK, x, a.nx, R(a.inX), R(a.inY), R(a.inZ), rho, ux,
                     uy, uz);
     vel[cell] = make_float4(float(ux), float(uy), float(uz), float(rho));
+    if (vel64) vel64[cell] = make_double4(double(ux), double(uy), double(uz), double(rho));
 }
 
 // Uniform equilibrium initialisation (lbm.c:670-721) of both buffers.
@@ -253,17 +369,25 @@ __global__ void __launch_bounds__(256) k_mass_momentum(const typename S::T *__re
 // ---------------------------------------------------------------------
 template <class S>
 struct StepLaunch {
-    static dim3 grid3(const GridImpl &g) {
-        return dim3((g.nx + g.bx - 1) / g.bx, (g.ny + g.by - 1) / g.by, g.nz);
+    static dim3 grid3(const GridImpl &g, int cpt = 1) {
+        const int wx = (g.nx + cpt - 1) / cpt;
+        return dim3((wx + g.bx - 1) / g.bx, (g.ny + g.by - 1) / g.by, g.nz);
     }
 
     template <int OP, bool SMAG>
     static void go(const GridImpl &g, const StepArgs &a, bool fused, cudaStream_t s) {
         const dim3 blk(g.bx, g.by, 1);
-        if (fused)
-            k_step<S, OP, SMAG, true><<<grid3(g), blk, 0, s>>>(a);
-        else
-            k_step<S, OP, SMAG, false><<<grid3(g), blk, 0, s>>>(a);
+        const int cpt = (g.cpt == 2 && g.nx % 2 == 0) ? 2 : 1;
+        if (fused) {
+            if (cpt == 2)
+                k_step<S, OP, SMAG, true, 2, 1><<<grid3(g, 2), blk, 0, s>>>(a);
+            else if (g.minb == 4)
+                k_step<S, OP, SMAG, true, 1, 4><<<grid3(g, 1), blk, 0, s>>>(a);
+            else
+                k_step<S, OP, SMAG, true, 1, 1><<<grid3(g, 1), blk, 0, s>>>(a);
+        } else {
+            k_step<S, OP, SMAG, false, 1, 1><<<grid3(g, 1), blk, 0, s>>>(a);
+        }
     }
 
     static cudaError_t step(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
@@ -285,8 +409,8 @@ struct StepLaunch {
     }
 
     static cudaError_t velocity(const GridImpl &g, const StepArgs &a, int kind, float4 *vel,
-                                cudaStream_t s) {
-        k_velocity<S><<<grid3(g), dim3(g.bx, g.by, 1), 0, s>>>(a, kind, vel);
+                                double4 *vel64, cudaStream_t s) {
+        k_velocity<S><<<grid3(g), dim3(g.bx, g.by, 1), 0, s>>>(a, kind, vel, vel64);
         return cudaGetLastError();
     }
 

@@ -296,7 +296,10 @@ def test_fp64_storage_matches_fp64_oracle(oracle, solver):
     gg.step(0.05, n=50)
     fo = og.f
     fg = gg.populations_f64()
-    assert S.rel_err(fg, fo) < 1e-12
+    err = S.rel_err(fg, fo)
+    print(f"fp64 storage vs fp64 oracle: max rel err {err:.3e}, "
+          f"bit-identical fraction {np.mean(fg == fo):.6f}")
+    assert err < 1e-12
     out, raw = gg.drag_force_f64()
     og.drag_force_decomposed()
     np.testing.assert_allclose(out, og.force_f64, rtol=1e-9, atol=1e-12)
