@@ -40,6 +40,17 @@ enum {
     LBM_STORAGE_FP64 = 3
 };
 
+/* Arithmetic of the step kernel (LBMGrid.arithmetic).  EXACT performs the
+ * reference shaders' operations as separately rounded IEEE single (or
+ * double) operations, bit-identical to the CPU oracle.  FAST contracts
+ * multiply-adds and uses hardware-approximate division and square root;
+ * its results stay within the parity tolerances of the tests but are not
+ * bit-identical.  FP64 storage always runs EXACT. */
+enum {
+    LBM_ARITH_EXACT = 0,
+    LBM_ARITH_FAST = 1
+};
+
 enum {
     LBM_OK = 0,
     LBM_ERR_INVALID_ARGUMENT = 1,
@@ -67,6 +78,7 @@ typedef struct LBMGrid {
     int periodicYZ;      /* 0 = clamp, 1 = periodic y/z          */
     /* extensions of this library */
     int storage;         /* LBM_STORAGE_*, fixed at creation     */
+    int arithmetic;      /* LBM_ARITH_*, may change between steps */
     int lastError;       /* last LBM_ERR_* code                  */
     void *impl;          /* opaque device state                  */
 } LBMGrid;

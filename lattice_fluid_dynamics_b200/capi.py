@@ -21,6 +21,8 @@ LBM_STORAGE_FP32 = 0
 LBM_STORAGE_FP16 = 1
 LBM_STORAGE_BF16 = 2
 LBM_STORAGE_FP64 = 3
+LBM_ARITH_EXACT = 0
+LBM_ARITH_FAST = 1
 STORAGE_NAMES = {"fp32": 0, "fp16": 1, "bf16": 2, "fp64": 3}
 
 
@@ -36,6 +38,7 @@ class LBMGrid(C.Structure):
         ("smagorinskyCs", C.c_float),
         ("periodicYZ", C.c_int),
         ("storage", C.c_int),
+        ("arithmetic", C.c_int),
         ("lastError", C.c_int),
         ("impl", C.c_void_p),
     ]

@@ -166,7 +166,9 @@ bool enqueue_step(LBMGrid *grid, float inX, float inY, float inZ) {
         a.src = I.pop[I.fbuf];
         a.dst = I.pop[I.gbuf];
         a.periodic = I.stream_periodic;
-        if (!ok(grid, launch_step(I, a, false, op, smag, I.stream))) return false;
+        if (!ok(grid, launch_step(I, a, false, op, smag, grid->arithmetic == LBM_ARITH_FAST,
+                                  I.stream)))
+            return false;
         I.vin = I.fbuf;
         I.vin_kind = IN_EXPLICIT_F;
         I.fbuf = -1;
@@ -175,7 +177,9 @@ bool enqueue_step(LBMGrid *grid, float inX, float inY, float inZ) {
         a.src = I.pop[src];
         a.dst = I.pop[dst];
         a.periodic = I.stream_periodic;
-        if (!ok(grid, launch_step(I, a, true, op, smag, I.stream))) return false;
+        if (!ok(grid, launch_step(I, a, true, op, smag, grid->arithmetic == LBM_ARITH_FAST,
+                                  I.stream)))
+            return false;
         I.vin = src;
         I.vin_kind = IN_POST_COLLISION;
         I.vin_periodic = I.stream_periodic;
@@ -264,6 +268,7 @@ LBMGrid *LBM_CreateEx(int sizeX, int sizeY, int sizeZ, float viscosity, int stor
     grid->smagorinskyCs = 0.1f;
     grid->periodicYZ = 0;
     grid->storage = storage;
+    grid->arithmetic = LBM_ARITH_EXACT;
     grid->lastError = LBM_OK;
 
     I->nx = sizeX;
@@ -497,7 +502,8 @@ void LBM_StepN(LBMGrid *grid, int nSteps, float inX, float inY, float inZ) {
         cv[2].f = inX;
         cv[3].f = inY;
         cv[4].f = inZ;
-        const int key[8] = {op_of(grid) * 4 + (grid->useSmagorinsky == 1) * 2 + grid->periodicYZ,
+        const int key[8] = {op_of(grid) * 8 + (grid->useSmagorinsky == 1) * 4 +
+                                grid->periodicYZ * 2 + (grid->arithmetic == LBM_ARITH_FAST),
                             cv[0].i, cv[1].i, cv[2].i, cv[3].i, cv[4].i, chunk, 1};
         const int par = I->gbuf;
         if (!I->graph[par] || memcmp(key, I->graph_key[par], sizeof(key)) != 0) {

@@ -16,7 +16,19 @@
 
 #include "lbm_internal.h"
 
+// Arithmetic flavour of the device code compiled in this translation unit:
+// `exact` (the default, --fmad=false and IEEE division/sqrt: the oracle's
+// rounding sequence) or `fast` (LBM_FAST_ARITH: contracted FMAs and
+// hardware-approximate division/sqrt).  Each flavour lives in its own
+// namespace so both can be linked into one library.
+#ifdef LBM_FAST_ARITH
+#define LBM_ARITH_NS fast
+#else
+#define LBM_ARITH_NS exact
+#endif
+
 namespace lbm {
+namespace LBM_ARITH_NS {
 
 // velocity set (lbm_collide.comp:33-52) and opposites (:76-77)
 __host__ __device__ constexpr int cx(int i) {
@@ -139,11 +151,19 @@ __device__ __forceinline__ R feq(int i, R rho, R ux, R uy, R uz) {
 }
 
 template <typename R> __device__ __forceinline__ R dsqrt(R v);
+#ifdef LBM_FAST_ARITH
+template <> __device__ __forceinline__ float dsqrt<float>(float v) { return sqrtf(v); }
+#else
 template <> __device__ __forceinline__ float dsqrt<float>(float v) { return __fsqrt_rn(v); }
+#endif
 template <> __device__ __forceinline__ double dsqrt<double>(double v) { return __dsqrt_rn(v); }
 
 template <typename R> __device__ __forceinline__ R ddiv(R a, R b);
+#ifdef LBM_FAST_ARITH
+template <> __device__ __forceinline__ float ddiv<float>(float a, float b) { return __fdividef(a, b); }
+#else
 template <> __device__ __forceinline__ float ddiv<float>(float a, float b) { return __fdiv_rn(a, b); }
+#endif
 template <> __device__ __forceinline__ double ddiv<double>(double a, double b) { return __ddiv_rn(a, b); }
 
 // Correctly rounded division by a constant y, given zh = RN(1/y):
@@ -159,9 +179,14 @@ template <> __device__ __forceinline__ double ddiv<double>(double a, double b) {
 template <typename R> __device__ __forceinline__ R cdiv(R x, R y, R zh);
 template <>
 __device__ __forceinline__ float cdiv<float>(float x, float y, float zh) {
+#ifdef LBM_FAST_ARITH
+    (void)y;
+    return x * zh;
+#else
     const float q1 = __fmul_rn(x, zh);
     const float r = __fmaf_rn(-q1, y, x);
     return __fmaf_rn(r, zh, q1);
+#endif
 }
 template <>
 __device__ __forceinline__ double cdiv<double>(double x, double y, double) {
@@ -509,4 +534,5 @@ __device__ __forceinline__ void collide(const R (&f)[19], R (&fn)[19], R rho, R 
     }
 }
 
+}  // namespace LBM_ARITH_NS
 }  // namespace lbm

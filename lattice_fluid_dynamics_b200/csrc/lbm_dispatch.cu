@@ -4,10 +4,11 @@
 
 namespace lbm {
 
-extern template struct StepLaunch<StoreF32>;
-extern template struct StepLaunch<StoreF64>;
-extern template struct StepLaunch<StoreF16>;
-extern template struct StepLaunch<StoreBF16>;
+using namespace exact;
+extern template struct exact::StepLaunch<exact::StoreF32>;
+extern template struct exact::StepLaunch<exact::StoreF64>;
+extern template struct exact::StepLaunch<exact::StoreF16>;
+extern template struct exact::StepLaunch<exact::StoreBF16>;
 
 #define LBM_DISPATCH(storage, CALL)                               \
     switch (storage) {                                            \
@@ -19,7 +20,9 @@ extern template struct StepLaunch<StoreBF16>;
     }
 
 cudaError_t launch_step(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
-                        cudaStream_t s) {
+                        bool fast_arith, cudaStream_t s) {
+    if (fast_arith && g.storage != LBM_STORAGE_FP64)
+        return fast::launch_step_fast(g, a, fused, op, smag, s);
     LBM_DISPATCH(g.storage, step(g, a, fused, op, smag, s));
 }
 

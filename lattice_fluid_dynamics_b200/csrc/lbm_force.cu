@@ -14,6 +14,8 @@
 
 namespace lbm {
 
+using namespace exact;
+
 namespace {
 
 struct ForceArgs {

@@ -15,6 +15,8 @@
 
 namespace lbm {
 
+using namespace exact;
+
 namespace {
 
 constexpr int TPB = 256;

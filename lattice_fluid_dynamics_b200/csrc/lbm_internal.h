@@ -99,7 +99,11 @@ struct StepArgs {
 
 // lbm_step.cu
 cudaError_t launch_step(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
-                        cudaStream_t s);
+                        bool fast_arith, cudaStream_t s);
+namespace fast {
+cudaError_t launch_step_fast(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
+                             cudaStream_t s);
+}
 cudaError_t launch_stream_only(const GridImpl &g, const void *src, void *dst, int periodic,
                                cudaStream_t s);
 cudaError_t launch_velocity(const GridImpl &g, const void *src, int kind, int periodic,

@@ -20,6 +20,7 @@
 #include "lbm_internal.h"
 
 namespace lbm {
+namespace LBM_ARITH_NS {
 
 // Row offsets of the y/z neighbours of a cell after the reference's
 // wrap (periodic) or clamp rule (lbm_stream.comp:63-74).
@@ -456,4 +457,5 @@ struct StepLaunch {
     }
 };
 
+}  // namespace LBM_ARITH_NS
 }  // namespace lbm

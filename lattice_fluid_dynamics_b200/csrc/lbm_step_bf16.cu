@@ -2,5 +2,5 @@
 #include "lbm_step.cuh"
 
 namespace lbm {
-template struct StepLaunch<StoreBF16>;
+template struct exact::StepLaunch<exact::StoreBF16>;
 }  // namespace lbm

@@ -2,5 +2,5 @@
 #include "lbm_step.cuh"
 
 namespace lbm {
-template struct StepLaunch<StoreF16>;
+template struct exact::StepLaunch<exact::StoreF16>;
 }  // namespace lbm

@@ -2,5 +2,5 @@
 #include "lbm_step.cuh"
 
 namespace lbm {
-template struct StepLaunch<StoreF32>;
+template struct exact::StepLaunch<exact::StoreF32>;
 }  // namespace lbm

@@ -2,5 +2,5 @@
 #include "lbm_step.cuh"
 
 namespace lbm {
-template struct StepLaunch<StoreF64>;
+template struct exact::StepLaunch<exact::StoreF64>;
 }  // namespace lbm
