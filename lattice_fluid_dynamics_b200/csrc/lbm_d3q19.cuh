@@ -203,6 +203,57 @@ template <> __device__ __forceinline__ double fmx<double>(double a, double b, do
     return __fma_rn(a, b, c);
 }
 
+// Paired single precision (sm_100 f32x2 add / sub / mul / fma): two
+// independent IEEE round-to-nearest operations per instruction, so every
+// lane is bit-identical to the scalar operation it replaces.  They are
+// issued as PTX with an explicit .rn modifier, which forbids the compiler
+// from contracting a paired multiply and add into one fused operation.
+__device__ __forceinline__ unsigned long long pbits(float2 a) {
+    return (unsigned long long)__float_as_uint(a.x) |
+           ((unsigned long long)__float_as_uint(a.y) << 32);
+}
+__device__ __forceinline__ float2 pfloat(unsigned long long d) {
+    return make_float2(__uint_as_float((unsigned)d), __uint_as_float((unsigned)(d >> 32)));
+}
+__device__ __forceinline__ float2 p2(float a, float b) { return make_float2(a, b); }
+// Operands pass through .b64 registers inside the asm block, so a constant
+// operand is moved as a bit pattern (an immediate on the arithmetic
+// instruction itself would be read as a number).
+__device__ __forceinline__ float2 padd(float2 a, float2 b) {
+    unsigned long long d;
+    asm("{\n\t.reg .b64 ra, rb;\n\tmov.b64 ra, %1;\n\tmov.b64 rb, %2;\n\t"
+        "add.rn.f32x2 %0, ra, rb;\n\t}"
+        : "=l"(d) : "l"(pbits(a)), "l"(pbits(b)));
+    return pfloat(d);
+}
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+    unsigned long long d;
+    asm("{\n\t.reg .b64 ra, rb;\n\tmov.b64 ra, %1;\n\tmov.b64 rb, %2;\n\t"
+        "sub.rn.f32x2 %0, ra, rb;\n\t}"
+        : "=l"(d) : "l"(pbits(a)), "l"(pbits(b)));
+    return pfloat(d);
+}
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) {
+    unsigned long long d;
+    asm("{\n\t.reg .b64 ra, rb;\n\tmov.b64 ra, %1;\n\tmov.b64 rb, %2;\n\t"
+        "mul.rn.f32x2 %0, ra, rb;\n\t}"
+        : "=l"(d) : "l"(pbits(a)), "l"(pbits(b)));
+    return pfloat(d);
+}
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) {
+    unsigned long long d;
+    asm("{\n\t.reg .b64 ra, rb, rc;\n\tmov.b64 ra, %1;\n\tmov.b64 rb, %2;\n\tmov.b64 rc, %3;\n\t"
+        "fma.rn.f32x2 %0, ra, rb, rc;\n\t}"
+        : "=l"(d) : "l"(pbits(a)), "l"(pbits(b)), "l"(pbits(c)));
+    return pfloat(d);
+}
+__device__ __forceinline__ float2 pneg(float2 a) { return make_float2(-a.x, -a.y); }
+// Measured on sm_100: a paired multiply whose result feeds a paired add or
+// subtract is contracted into one fused operation even with explicit .rn,
+// and so are pairs of scalar multiplies the compiler merges.  Paired
+// arithmetic is therefore used only where no product feeds a paired sum:
+// sums, and fused operations whose products are exact or intended.
+
 // Zou-He boundaries (lbm_collide.comp:336-408); rewrite f in place.
 template <typename R>
 __device__ __forceinline__ void zou_he_inlet(R (&f)[19], R ux, R uy, R uz) {
@@ -351,6 +402,111 @@ __device__ __forceinline__ void mrt_inverse(const R (&m)[19], R (&fi)[19]) {
     ms[18] = m[18] * R(0.125);
 
     // lbm_collide.comp:210-310, left to right; products by 2, 4, 8 fused
+#if !defined(LBM_FAST_ARITH) && !defined(LBM_NO_PAIRED)
+    if constexpr (sizeof(R) == 4) {
+        // Populations in pairs (i, j) whose sums take the same operands in
+        // the same order with per-lane signs: each step is one paired
+        // fma with a sign pair in {+-1, +-2, +-4} (exact products), i.e.
+        // the scalar add or subtract of the shader on both lanes.
+        float2 B[19];
+#pragma unroll
+        for (int k = 0; k < 19; k++) B[k] = p2(ms[k], ms[k]);
+        auto S = [](float a, float b) { return p2(a, b); };
+        fi[0] = (ms[0] - R(30) * ms[1]) + R(12) * ms[2];
+        const float a0 = fmx<R>(R(-4), ms[2], ms[0] - R(11) * ms[1]);
+        const float b0 = fmx<R>(R(8), ms[1], ms[0]) + ms[2];
+        const float2 A0 = p2(a0, a0), B0 = p2(b0, b0);
+        float2 P;
+        P = pfma(S(1, -1), B[3], A0);
+        P = pfma(S(-4, 4), B[4], P);
+        P = pfma(S(2, 2), B[9], P);
+        P = pfma(S(-4, -4), B[10], P);
+        fi[1] = P.x, fi[2] = P.y;
+        P = pfma(S(1, -1), B[5], A0);
+        P = pfma(S(-4, 4), B[6], P);
+        P = psub(P, B[9]);
+        P = pfma(S(2, 2), B[10], P);
+        P = padd(P, B[11]);
+        P = pfma(S(-2, -2), B[12], P);
+        fi[3] = P.x, fi[4] = P.y;
+        P = pfma(S(1, -1), B[7], A0);
+        P = pfma(S(-4, 4), B[8], P);
+        P = psub(P, B[9]);
+        P = pfma(S(2, 2), B[10], P);
+        P = psub(P, B[11]);
+        P = pfma(S(2, 2), B[12], P);
+        fi[5] = P.x, fi[6] = P.y;
+        P = pfma(S(1, -1), B[3], B0);  // 7, 8
+        P = pfma(S(1, -1), B[4], P);
+        P = padd(P, B[5]);
+        P = padd(P, B[6]);
+        P = padd(P, B[9]);
+        P = padd(P, B[10]);
+        P = padd(P, B[11]);
+        P = padd(P, B[12]);
+        P = pfma(S(1, -1), B[13], P);
+        P = pfma(S(1, -1), B[16], P);
+        P = psub(P, B[17]);
+        fi[7] = P.x, fi[8] = P.y;
+        P = pfma(S(1, -1), B[3], B0);  // 9, 10
+        P = pfma(S(1, -1), B[4], P);
+        P = psub(P, B[5]);
+        P = psub(P, B[6]);
+        P = padd(P, B[9]);
+        P = padd(P, B[10]);
+        P = padd(P, B[11]);
+        P = padd(P, B[12]);
+        P = pfma(S(-1, 1), B[13], P);
+        P = pfma(S(1, -1), B[16], P);
+        P = padd(P, B[17]);
+        fi[9] = P.x, fi[10] = P.y;
+        P = pfma(S(1, -1), B[3], B0);  // 11, 12
+        P = pfma(S(1, -1), B[4], P);
+        P = padd(P, B[7]);
+        P = padd(P, B[8]);
+        P = padd(P, B[9]);
+        P = padd(P, B[10]);
+        P = psub(P, B[11]);
+        P = psub(P, B[12]);
+        P = pfma(S(1, -1), B[15], P);
+        P = pfma(S(-1, 1), B[16], P);
+        P = padd(P, B[18]);
+        fi[11] = P.x, fi[12] = P.y;
+        P = pfma(S(1, -1), B[3], B0);  // 13, 14
+        P = pfma(S(1, -1), B[4], P);
+        P = psub(P, B[7]);
+        P = psub(P, B[8]);
+        P = padd(P, B[9]);
+        P = padd(P, B[10]);
+        P = psub(P, B[11]);
+        P = psub(P, B[12]);
+        P = pfma(S(-1, 1), B[15], P);
+        P = pfma(S(-1, 1), B[16], P);
+        P = psub(P, B[18]);
+        fi[13] = P.x, fi[14] = P.y;
+        P = pfma(S(1, -1), B[5], B0);  // 15, 16
+        P = pfma(S(1, -1), B[6], P);
+        P = padd(P, B[7]);
+        P = padd(P, B[8]);
+        P = pfma(S(-2, -2), B[9], P);
+        P = pfma(S(-2, -2), B[10], P);
+        P = pfma(S(1, -1), B[14], P);
+        P = pfma(S(1, -1), B[17], P);
+        P = psub(P, B[18]);
+        fi[15] = P.x, fi[16] = P.y;
+        P = pfma(S(1, -1), B[5], B0);  // 17, 18
+        P = pfma(S(1, -1), B[6], P);
+        P = psub(P, B[7]);
+        P = psub(P, B[8]);
+        P = pfma(S(-2, -2), B[9], P);
+        P = pfma(S(-2, -2), B[10], P);
+        P = pfma(S(-1, 1), B[14], P);
+        P = pfma(S(1, -1), B[17], P);
+        P = padd(P, B[18]);
+        fi[17] = P.x, fi[18] = P.y;
+        return;
+    }
+#endif
     fi[0] = (ms[0] - R(30) * ms[1]) + R(12) * ms[2];
     const R a0 = fmx<R>(R(-4), ms[2], ms[0] - R(11) * ms[1]);  // ms0 - 11ms1 - 4ms2
     fi[1] = fmx<R>(R(-4), ms[10], fmx<R>(R(2), ms[9], fmx<R>(R(-4), ms[4], a0 + ms[3])));
@@ -414,6 +570,42 @@ __device__ __forceinline__ void equilibria(R rho, R ux, R uy, R uz, R (&fe)[19])
         fi = wr * (((R(1) + a) + b) - cu);
         fj = wr * (((R(1) - a) + b) - cu);
     };
+#if !defined(LBM_FAST_ARITH) && !defined(LBM_NO_PAIRED)
+    if constexpr (sizeof(R) == 4) {
+        // two direction pairs per paired instruction; lane k evaluates the
+        // scalar sequence of `pair` above.  Only sums and fused operations
+        // of the Markstein quotient are paired: a paired product that feeds
+        // a paired sum is contracted by the compiler (measured on sm_100).
+        const float2 ONE = p2(1.0f, 1.0f), CU = p2(cu, cu);
+        const float2 Y1 = p2(cs2, cs2), Z1 = p2(1.0f / cs2, 1.0f / cs2);
+        const float2 Y2 = p2(c2, c2), Z2 = p2(1.0f / c2, 1.0f / c2);
+        auto lanes = [&](float e0, float e1, float w0, float w1, float &fi0, float &fj0,
+                         float &fi1, float &fj1) {
+            const float2 E = p2(e0, e1);
+            const float2 E2 = pmul(E, E);
+            // Markstein: q1 = RN(x zh); r = fma(-q1, y, x); q = fma(r, zh, q1)
+            const float2 q1a = pmul(E, Z1);
+            const float2 ra = pfma(pneg(q1a), Y1, E);
+            const float2 a = pfma(ra, Z1, q1a);
+            const float2 q1b = pmul(E2, Z2);
+            const float2 rb = pfma(pneg(q1b), Y2, E2);
+            const float2 b = pfma(rb, Z2, q1b);
+            const float2 Si = psub(padd(padd(ONE, a), b), CU);
+            const float2 Sj = psub(padd(psub(ONE, a), b), CU);
+            // the products by w rho stay scalar: they feed subtractions
+            fi0 = __fmul_rn(w0, Si.x);
+            fi1 = __fmul_rn(w1, Si.y);
+            fj0 = __fmul_rn(w0, Sj.x);
+            fj1 = __fmul_rn(w1, Sj.y);
+        };
+        lanes(ux, uy, wr1, wr1, fe[1], fe[2], fe[3], fe[4]);
+        lanes(uz, ux + uy, wr1, wr2, fe[5], fe[6], fe[7], fe[10]);
+        lanes(uy - ux, ux + uz, wr2, wr2, fe[8], fe[9], fe[11], fe[14]);
+        lanes(uz - ux, uy + uz, wr2, wr2, fe[12], fe[13], fe[15], fe[18]);
+        pair(uz - uy, wr2, fe[16], fe[17]);
+        return;
+    }
+#endif
     pair(ux, wr1, fe[1], fe[2]);
     pair(uy, wr1, fe[3], fe[4]);
     pair(uz, wr1, fe[5], fe[6]);
@@ -486,8 +678,10 @@ __device__ __forceinline__ void collide(const R (&f)[19], R (&fn)[19], R rho, R 
         Q[12] = Q[13] = fmx<R>(R(-2), Pxz, Txz);
         Q[15] = Q[18] = fmx<R>(R(2), Pyz, Tyz);
         Q[16] = Q[17] = fmx<R>(R(-2), Pyz, Tyz);
+        {
 #pragma unroll
-        for (int i = 0; i < 19; i++) fn[i] = fe[i] + om * ((wgt<R>(i) * R(4.5)) * Q[i]);
+            for (int i = 0; i < 19; i++) fn[i] = fe[i] + om * ((wgt<R>(i) * R(4.5)) * Q[i]);
+        }
     } else if (OP == OP_MRT) {
         // :550-616
         R m[19], meq[19];
@@ -511,26 +705,30 @@ __device__ __forceinline__ void collide(const R (&f)[19], R (&fn)[19], R rho, R 
         const R s_nu = omega;
         // relaxation m - s (m - meq); the conserved moments 0, 3, 5, 7 have
         // s = 0 and keep their value; meq of the ghost modes 16-18 is 0
-        m[1] = m[1] - R(1.19) * (m[1] - meq[1]);
-        m[2] = m[2] - R(1.4) * (m[2] - meq[2]);
-        m[4] = m[4] - R(1.2) * (m[4] - meq[4]);
-        m[6] = m[6] - R(1.2) * (m[6] - meq[6]);
-        m[8] = m[8] - R(1.2) * (m[8] - meq[8]);
-        m[9] = m[9] - s_nu * (m[9] - meq[9]);
-        m[10] = m[10] - R(1.4) * (m[10] - meq[10]);
-        m[11] = m[11] - s_nu * (m[11] - meq[11]);
-        m[12] = m[12] - R(1.4) * (m[12] - meq[12]);
-        m[13] = m[13] - s_nu * (m[13] - meq[13]);
-        m[14] = m[14] - s_nu * (m[14] - meq[14]);
-        m[15] = m[15] - s_nu * (m[15] - meq[15]);
-        m[16] = m[16] - R(1.98) * m[16];
-        m[17] = m[17] - R(1.98) * m[17];
-        m[18] = m[18] - R(1.98) * m[18];
+        {
+            m[1] = m[1] - R(1.19) * (m[1] - meq[1]);
+            m[2] = m[2] - R(1.4) * (m[2] - meq[2]);
+            m[4] = m[4] - R(1.2) * (m[4] - meq[4]);
+            m[6] = m[6] - R(1.2) * (m[6] - meq[6]);
+            m[8] = m[8] - R(1.2) * (m[8] - meq[8]);
+            m[9] = m[9] - s_nu * (m[9] - meq[9]);
+            m[10] = m[10] - R(1.4) * (m[10] - meq[10]);
+            m[11] = m[11] - s_nu * (m[11] - meq[11]);
+            m[12] = m[12] - R(1.4) * (m[12] - meq[12]);
+            m[13] = m[13] - s_nu * (m[13] - meq[13]);
+            m[14] = m[14] - s_nu * (m[14] - meq[14]);
+            m[15] = m[15] - s_nu * (m[15] - meq[15]);
+            m[16] = m[16] - R(1.98) * m[16];
+            m[17] = m[17] - R(1.98) * m[17];
+            m[18] = m[18] - R(1.98) * m[18];
+        }
         mrt_inverse<R>(m, fn);
     } else {
         // :618-625
+        {
 #pragma unroll
-        for (int i = 0; i < 19; i++) fn[i] = f[i] - omega * (f[i] - fe[i]);
+            for (int i = 0; i < 19; i++) fn[i] = f[i] - omega * (f[i] - fe[i]);
+        }
     }
 }
 

@@ -191,15 +191,19 @@ __global__ void __launch_bounds__(256, MINB) k_step(const StepArgs a) {
     if (FUSED) {
         const bool interior = x0 > 0 && x0 + CPT < a.nx && y > 0 && y + 1 < a.ny && z > 0 &&
                               z + 1 < a.nz;
-        const Rows rw = neighbour_rows(a, y, z);
         if (interior) {
             gather_interior<S, CPT>(a, src, cell0, cur, nxt);
         } else {
+            const Rows rw = neighbour_rows(a, y, z);
             gather_pull<S>(a, src, x0, rw, cell0, cur);
             if (CPT == 2) gather_pull<S>(a, src, x0 + 1, rw, cell0 + 1, nxt);
         }
-        if (flag0 & FLAG_BOUNDARY) bouzidi<S>(a, src, x0, rw, cell0, cur);
-        if (CPT == 2 && (flag1 & FLAG_BOUNDARY)) bouzidi<S>(a, src, x0 + 1, rw, cell0 + 1, nxt);
+        if ((flag0 | flag1) & FLAG_BOUNDARY) {
+            const Rows rw = neighbour_rows(a, y, z);
+            if (flag0 & FLAG_BOUNDARY) bouzidi<S>(a, src, x0, rw, cell0, cur);
+            if (CPT == 2 && (flag1 & FLAG_BOUNDARY))
+                bouzidi<S>(a, src, x0 + 1, rw, cell0 + 1, nxt);
+        }
     } else {
 #pragma unroll
         for (int i = 0; i < 19; i++) {
