@@ -303,12 +303,12 @@ def main():
 
     if rank == 0:
         traffic = None
-        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        tpath = os.path.join(ROOT, "profiles", "dram_traffic_per_launch.txt")
         if os.path.exists(tpath):
-            try:
-                traffic = json.load(open(tpath)).get(WORKLOAD)
-            except Exception:
-                traffic = None
+            for line in open(tpath):
+                parts = line.split()
+                if len(parts) == 2 and parts[0] == WORKLOAD:
+                    traffic = int(parts[1])
         line = {
             "metric": "MLUPS", "value": round(mlups, 2), "unit": "MLUPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
