@@ -219,6 +219,22 @@ int LBM_ComputeDragForceF64(LBMGrid *grid, double *out6, long long *raw7);
  * out[0] = mass (sum of rho), out[1..3] = momentum. */
 int LBM_ComputeMassMomentum(LBMGrid *grid, double *out4);
 
+/* No counterpart in the reference.  FP64 mass and momentum (out4[0] =
+ * sum of rho, out4[1..3] = momentum) of a caller-owned FP32 population field
+ * in this library's SoA layout, populations[i * numCells + cell], on
+ * `stream` (a cudaStream_t; NULL is the legacy default stream), written to
+ * host memory out4 after the stream is synchronised.  It allocates nothing,
+ * for callers that cannot call cudaMalloc (graph capture or replay, real-time
+ * loops, memory owned by another allocator): the scratch is a fixed 128 KiB
+ * __device__ array held per GPU for the life of the process, which limits
+ * numCells to 268,435,456 (larger fields return LBM_ERR_INVALID_ARGUMENT).
+ * The first call on each device looks up that array's device address
+ * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU race.  Returns LBM_OK or an
+ * LBM_ERR_* code. */
+int LBM_MassMomentumNoAlloc(const float *populations, long long numCells,
+                            double *out4, void *stream);
+
 /* Cells reset by the stability guard since LBM_InitializeFlow. */
 long long LBM_GetGuardResetCount(LBMGrid *grid);
 

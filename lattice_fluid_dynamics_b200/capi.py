@@ -85,6 +85,7 @@ SIGNATURES = {
     "LBM_ComputeDragForceF64": (C.c_int, [_G, _vp, _vp]),
     "LBM_ComputeMassMomentum": (C.c_int, [_G, _vp]),
     "LBM_GetGuardResetCount": (C.c_longlong, [_G]),
+    "LBM_MassMomentumNoAlloc": (C.c_int, [_vp, C.c_longlong, _vp, _vp]),
     "LBM_LoadPopulations": (C.c_int, [_G, _vp]),
     "LBM_InitializeFromField": (C.c_int, [_G, _vp, _vp]),
     "LBM_GetLastError": (C.c_int, [_G]),
