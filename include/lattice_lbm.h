@@ -272,6 +272,61 @@ int LBM_ParticlesLoad(LBMParticles *p, const LBMParticle *host);
 /* device pointer to the LBMParticle array */
 void *LBM_ParticlesDevice(LBMParticles *p);
 
+/* ---------------------------------------------------------------------
+ * Host side of the driver: OBJ ingestion, model placement, Re -> tau,
+ * Strouhal number.  Plain C on the host, no device work.
+ * ------------------------------------------------------------------- */
+
+/* Same layout as the reference's Model (obj-file-loader/lib/model_loader.h:
+ * 4-18): vertices x,y,z per vertex, faces three 1-based indices per face. */
+typedef struct {
+    float *vertices;
+    int *faces;
+    int vertexCount;
+    int faceCount;
+} LBMModel;
+
+/* Replaces loadOBJ (obj-file-loader/lib/model_loader.c:54-151): "v x y z"
+ * lines, "f a b c" lines in any of v, v/vt, v/vt/vn, v//vn; only the first
+ * three references of a face are kept.  Returns 1, or 0 when the file
+ * cannot be opened. */
+int LBM_LoadOBJ(const char *path, LBMModel *model);
+/* Replaces freeModel (model_loader.c:153-160). */
+void LBM_FreeModel(LBMModel *model);
+
+/* Replaces computeModelBounds (src/model_bounds.c:146-209): bounds9 =
+ * {minX,minY,minZ, maxX,maxY,maxZ, centerX,centerY,centerZ} of the
+ * vertices scaled, offset and rotated by rotationY degrees about y. */
+int LBM_ModelBounds(const LBMModel *model, float scale, float offsetX, float offsetY,
+                    float offsetZ, float rotationY, float *bounds9);
+
+/* Replaces createTriangleBuffer (src/model_bounds.c:211-287): 12 floats per
+ * valid face (three xyz+pad vertices, the layout LBM_SetSolidMesh takes);
+ * faces with an index out of range are skipped.  Free with
+ * LBM_FreeTriangles. */
+float *LBM_CreateTriangleBuffer(const LBMModel *model, float scale, float offsetX,
+                                float offsetY, float offsetZ, float rotationY,
+                                int *outCount);
+void LBM_FreeTriangles(float *triangles);
+
+/* The placement main.c applies after loading (src/main.c:250-349): scale
+ * 2.4 / largest raw extent unless scaleOrZero > 0, centre at the origin,
+ * rotate 90 degrees about y when z is longer than x, centre at x = -2. */
+int LBM_PlaceModel(const LBMModel *model, float scaleOrZero, float *scale, float *offset3,
+                   float *rotationY);
+
+/* src/main.c:447-460: nu = U L / Re, tau = 3 nu + 0.5, clamped at 0.52
+ * (then Re = U L / nu).  Returns 1, 2 when clamped, 0 on bad arguments. */
+int LBM_ReynoldsToTau(float latticeVelocity, float charLength, float reynolds, float *tau,
+                      float *viscosity, float *effectiveReynolds);
+
+/* Replaces compute_strouhal (src/drag_metrics.c:8-68) with the sample
+ * interval as an argument (CD_SAMPLE_INTERVAL = 20 in the reference) and
+ * the result returned instead of printed: St = f_peak L / U from a
+ * Hann-windowed DFT of the last 65 % of the Cl series. */
+float LBM_Strouhal(const float *clSeries, int clCount, int lbmSubsteps, int sampleInterval,
+                   float charLength, float latticeVelocity, float *peakFrequency);
+
 #ifdef __cplusplus
 }
 #endif

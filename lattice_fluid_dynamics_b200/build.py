@@ -1,6 +1,6 @@
 """Build the sm_100a solver library ``liblattice_lbm.so`` in-tree.
 
-Every .cu file under csrc/ is compiled by nvcc for sm_100a
+Every .cu (and host-only .cpp) file under csrc/ is compiled by nvcc for sm_100a
 (``-gencode arch=compute_100a,code=sm_100a``) with ``--fmad=false`` and the
 default IEEE division / square root, so that single-precision arithmetic
 rounds exactly as the C oracle (built with -ffp-contract=off) does; the
@@ -28,7 +28,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-prec-div=true",
 
 def sources():
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC)
-                  if f.endswith(".cu"))
+                  if f.endswith((".cu", ".cpp")))
 
 
 def _headers_mtime():

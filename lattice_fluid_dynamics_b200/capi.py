@@ -44,6 +44,12 @@ class LBMGrid(C.Structure):
     ]
 
 
+class LBMModel(C.Structure):
+    """Mirror of ``LBMModel`` (the reference's Model, obj-file-loader/lib/model_loader.h:4-18)."""
+    _fields_ = [("vertices", C.POINTER(C.c_float)), ("faces", C.POINTER(C.c_int)),
+                ("vertexCount", C.c_int), ("faceCount", C.c_int)]
+
+
 class LBMParticle(C.Structure):
     _fields_ = [(n, C.c_float) for n in
                 ("x", "y", "z", "pad", "vx", "vy", "vz", "life")]
@@ -97,6 +103,14 @@ SIGNATURES = {
     "LBM_ParticlesCopy": (C.c_int, [_vp, _vp]),
     "LBM_ParticlesLoad": (C.c_int, [_vp, _vp]),
     "LBM_ParticlesDevice": (_vp, [_vp]),
+    "LBM_LoadOBJ": (C.c_int, [C.c_char_p, _vp]),
+    "LBM_FreeModel": (None, [_vp]),
+    "LBM_ModelBounds": (C.c_int, [_vp, _f, _f, _f, _f, _f, _vp]),
+    "LBM_CreateTriangleBuffer": (_vp, [_vp, _f, _f, _f, _f, _f, _vp]),
+    "LBM_FreeTriangles": (None, [_vp]),
+    "LBM_PlaceModel": (C.c_int, [_vp, _f, _vp, _vp, _vp]),
+    "LBM_ReynoldsToTau": (C.c_int, [_f, _f, _f, _vp, _vp, _vp]),
+    "LBM_Strouhal": (_f, [_vp, C.c_int, C.c_int, C.c_int, _f, _f, _vp]),
 }
 
 _lib = None
@@ -342,3 +356,94 @@ class Particles:
     def set(self, arr: np.ndarray):
         arr = np.ascontiguousarray(arr, np.float32).reshape(self.n, 8)
         assert self._L.LBM_ParticlesLoad(self._p, _p(arr)) == 1
+
+
+class Model:
+    """An OBJ model loaded by LBM_LoadOBJ (reference loadOBJ semantics)."""
+
+    def __init__(self, path: str):
+        self._L = load()
+        self._m = LBMModel()
+        if self._L.LBM_LoadOBJ(os.fsencode(path), C.byref(self._m)) != 1:
+            raise OSError(f"LBM_LoadOBJ could not open {path}")
+
+    def close(self):
+        if getattr(self, "_m", None) is not None:
+            self._L.LBM_FreeModel(C.byref(self._m))
+            self._m = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def vertex_count(self) -> int:
+        return self._m.vertexCount
+
+    @property
+    def face_count(self) -> int:
+        return self._m.faceCount
+
+    def vertices(self) -> np.ndarray:
+        n = self._m.vertexCount
+        if n == 0:
+            return np.zeros((0, 3), np.float32)
+        return np.ctypeslib.as_array(self._m.vertices, (n, 3)).copy()
+
+    def faces(self) -> np.ndarray:
+        n = self._m.faceCount
+        if n == 0:
+            return np.zeros((0, 3), np.int32)
+        return np.ctypeslib.as_array(self._m.faces, (n, 3)).copy()
+
+    def place(self, scale: float = 0.0):
+        """(scale, (ox, oy, oz), rotationY) as the reference's main.c places a model."""
+        s = C.c_float()
+        off = (C.c_float * 3)()
+        rot = C.c_float()
+        if self._L.LBM_PlaceModel(C.byref(self._m), scale, C.byref(s), off, C.byref(rot)) != 1:
+            raise ValueError("LBM_PlaceModel: empty model")
+        return s.value, (off[0], off[1], off[2]), rot.value
+
+    def bounds(self, scale, offset, rotation_y) -> np.ndarray:
+        out = np.empty(9, np.float32)
+        self._L.LBM_ModelBounds(C.byref(self._m), scale, *offset, rotation_y, _p(out))
+        return out
+
+    def triangles(self, scale, offset, rotation_y) -> np.ndarray:
+        """(n, 12) float32 triangle buffer for LBM_SetSolidMesh."""
+        cnt = C.c_int()
+        ptr = self._L.LBM_CreateTriangleBuffer(C.byref(self._m), scale, *offset, rotation_y,
+                                               C.byref(cnt))
+        if not ptr:
+            return np.zeros((0, 12), np.float32)
+        try:
+            arr = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_float)),
+                                        (cnt.value, 12)).copy()
+        finally:
+            self._L.LBM_FreeTriangles(ptr)
+        return arr
+
+
+def reynolds_to_tau(lattice_velocity: float, char_length: float, reynolds: float):
+    """(tau, viscosity, effective_reynolds, clamped) by the reference's rule."""
+    L = load()
+    t, nu, re = C.c_float(), C.c_float(), C.c_float()
+    rc = L.LBM_ReynoldsToTau(lattice_velocity, char_length, reynolds, C.byref(t),
+                             C.byref(nu), C.byref(re))
+    if rc == 0:
+        raise ValueError("LBM_ReynoldsToTau: bad arguments")
+    return t.value, nu.value, re.value, rc == 2
+
+
+def strouhal(cl_series, lbm_substeps: int, char_length: float, lattice_velocity: float,
+             sample_interval: int = 20):
+    """(St, peak frequency) of a Cl series, the reference's compute_strouhal."""
+    L = load()
+    cl = np.ascontiguousarray(cl_series, np.float32)
+    f = C.c_float()
+    st = L.LBM_Strouhal(_p(cl), len(cl), lbm_substeps, sample_interval, char_length,
+                        lattice_velocity, C.byref(f))
+    return st, f.value
