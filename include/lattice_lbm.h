@@ -327,6 +327,92 @@ int LBM_ReynoldsToTau(float latticeVelocity, float charLength, float reynolds, f
 float LBM_Strouhal(const float *clSeries, int clCount, int lbmSubsteps, int sampleInterval,
                    float charLength, float latticeVelocity, float *peakFrequency);
 
+/* ---------------------------------------------------------------------
+ * Headless wind-tunnel driver: the solver loop of the reference's main()
+ * without rendering (src/main.c:438-553, 893-1391).  Its stdout lines keep
+ * the reference's formats, so scripts that scrape the reference's binary
+ * (modal_worker.py:474-560, test/benchmark.sh:57-79) read it unchanged.
+ * ------------------------------------------------------------------- */
+#define LBM_CD_SAMPLE_INTERVAL 20 /* frames between Cd samples (drag_metrics.h:5) */
+#define LBM_CD_HISTORY_SIZE 100   /* samples in the convergence window (drag_metrics.h:4) */
+#define LBM_RAMP_FRAMES 300       /* inlet ramp length in frames (main.c:944) */
+
+/* Cd convergence monitor (main.c:1309-1391): EMA of the corrected Cd
+ * (alpha 0.1, seeded while no sample has been accepted), ring of the last
+ * 100 accepted Cd values (0 < Cd < 1000), converged once their relative
+ * standard deviation drops below 1 %. */
+typedef struct {
+    float history[LBM_CD_HISTORY_SIZE];
+    int historyCount;
+    int converged;
+    float ema;
+    float convergedMean;
+    float convergedRelStd;
+} LBMCdMonitor;
+
+void LBM_CdMonitorInit(LBMCdMonitor *m);
+/* Add one sample; returns 1 when this sample made the series converge. */
+int LBM_CdMonitorAdd(LBMCdMonitor *m, float cd, float cdCorr);
+
+/* Coefficients of one sample (main.c:1256-1270): dynamic pressure
+ * 0.5 rho0 U^2 with rho0 = 1, Cd = |Fx| / (q A), Cl = Fy / (q A) (signed),
+ * Cd_pressure = |Px| / (q A), Cd_friction = max(Cd - Cd_pressure, 0),
+ * Cd_corr = Cd * blockageFactor. */
+typedef struct {
+    float cd, cdCorr, cl, cdPressure, cdFriction;
+} LBMCoefficients;
+void LBM_TunnelCoefficients(float fx, float fy, float px, float latticeVelocity, float refArea,
+                            float blockageFactor, LBMCoefficients *out);
+
+/* First frame that samples Cd (main.c:968-981): 300 ramp frames plus three
+ * flow-throughs, pulled back to 2/3 of a short run's frame budget. */
+int LBM_TunnelCdStartFrame(int sizeX, float latticeVelocity, int substeps, int maxFrames);
+
+/* Inlet ramp factor of a frame (main.c:944-947): frame / 300, then 1. */
+float LBM_TunnelRampFactor(int frame);
+
+typedef struct {
+    const char *modelPath;   /* OBJ file; NULL or "" = no mesh (AABB fallback box) */
+    float windSpeed;         /* 0-5; Re = 200 * wind (at least 50) when reynolds <= 0 */
+    int renderDuration;      /* seconds of output at 60 frames/s (> 0) */
+    float reynolds;          /* <= 0: derived from windSpeed */
+    float scale;             /* <= 0: auto scale 2.4 / largest extent */
+    int gridX, gridY, gridZ; /* 128 x 64 x 64 in the reference */
+    float smagorinskyCs;     /* 0.1 in the reference */
+    int substeps;            /* lattice steps per frame, 10 in the reference */
+    float latticeVelocity;   /* 0.05 in the reference */
+    const char *vtkOutputPath; /* NULL or "": no VTI dumps */
+    int vtkInterval;         /* frames between VTI dumps */
+    const char *logPath;     /* NULL or "": stdout; else the lines go to this file */
+    int storage;             /* LBM_STORAGE_* of the populations */
+} LBMTunnelOptions;
+
+/* The reference's defaults (cli.c:12-39, main.c:59,434). */
+void LBM_TunnelDefaults(LBMTunnelOptions *o);
+
+typedef struct {
+    int frames;              /* frames run */
+    long long latticeSteps;  /* frames * substeps */
+    int cdSamples;           /* Cd lines printed */
+    int cdStartFrame;
+    float tau, viscosity, reynolds, charLength;
+    float refArea, blockage, blockageFactor;
+    float lastCd, lastCdCorr, lastCl, cdEma;
+    int converged;
+    float convergedMean;
+    float strouhal, sheddingFrequency;
+    double seconds;          /* wall time of the frame loop */
+    double mlups;            /* lattice updates / s / 1e6 over the frame loop */
+    int solidCells;
+    int triangles;
+} LBMTunnelResult;
+
+/* Run the headless loop: load and place the model, set the mesh, Re -> tau,
+ * MRT + Smagorinsky + periodic y/z, ramped inlet, Cd every 20 frames after
+ * the start frame, EMA and convergence (which shortens the run to 120 more
+ * frames), Strouhal at the end.  Returns LBM_OK or an LBM_ERR_* code. */
+int LBM_TunnelRun(const LBMTunnelOptions *options, LBMTunnelResult *result);
+
 #ifdef __cplusplus
 }
 #endif

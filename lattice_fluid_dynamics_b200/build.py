@@ -18,6 +18,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "liblattice_lbm.so")
+TUNNEL = os.path.join(HERE, "lattice_tunnel")
+TUNNEL_SRC = os.path.join(HERE, "driver", "lattice_tunnel.c")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -75,6 +77,15 @@ def build(verbose_ptxas: bool = False, jobs: int | None = None) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    if (not os.path.exists(TUNNEL) or os.path.getmtime(TUNNEL) < os.path.getmtime(LIB)
+            or os.path.getmtime(TUNNEL) < os.path.getmtime(TUNNEL_SRC)):
+        # the headless driver executable, linked against the library beside it
+        cmd = ["gcc", "-O2", "-std=gnu11", "-Wall", "-I" + os.path.join(HERE, "..", "include"),
+               "-o", TUNNEL, TUNNEL_SRC, "-L" + HERE, "-llattice_lbm",
+               "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"driver build failed:\n{r.stdout}\n{r.stderr}")
     return LIB
 
 

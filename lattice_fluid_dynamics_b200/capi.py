@@ -50,6 +50,36 @@ class LBMModel(C.Structure):
                 ("vertexCount", C.c_int), ("faceCount", C.c_int)]
 
 
+class LBMCdMonitor(C.Structure):
+    _fields_ = [("history", C.c_float * 100), ("historyCount", C.c_int), ("converged", C.c_int),
+                ("ema", C.c_float), ("convergedMean", C.c_float),
+                ("convergedRelStd", C.c_float)]
+
+
+class LBMCoefficients(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("cd", "cdCorr", "cl", "cdPressure", "cdFriction")]
+
+
+class LBMTunnelOptions(C.Structure):
+    _fields_ = [("modelPath", C.c_char_p), ("windSpeed", C.c_float),
+                ("renderDuration", C.c_int), ("reynolds", C.c_float), ("scale", C.c_float),
+                ("gridX", C.c_int), ("gridY", C.c_int), ("gridZ", C.c_int),
+                ("smagorinskyCs", C.c_float), ("substeps", C.c_int),
+                ("latticeVelocity", C.c_float), ("vtkOutputPath", C.c_char_p),
+                ("vtkInterval", C.c_int), ("logPath", C.c_char_p), ("storage", C.c_int)]
+
+
+class LBMTunnelResult(C.Structure):
+    _fields_ = [("frames", C.c_int), ("latticeSteps", C.c_longlong), ("cdSamples", C.c_int),
+                ("cdStartFrame", C.c_int)] + \
+               [(n, C.c_float) for n in ("tau", "viscosity", "reynolds", "charLength",
+                                         "refArea", "blockage", "blockageFactor", "lastCd",
+                                         "lastCdCorr", "lastCl", "cdEma")] + \
+               [("converged", C.c_int), ("convergedMean", C.c_float), ("strouhal", C.c_float),
+                ("sheddingFrequency", C.c_float), ("seconds", C.c_double),
+                ("mlups", C.c_double), ("solidCells", C.c_int), ("triangles", C.c_int)]
+
+
 class LBMParticle(C.Structure):
     _fields_ = [(n, C.c_float) for n in
                 ("x", "y", "z", "pad", "vx", "vy", "vz", "life")]
@@ -111,6 +141,13 @@ SIGNATURES = {
     "LBM_PlaceModel": (C.c_int, [_vp, _f, _vp, _vp, _vp]),
     "LBM_ReynoldsToTau": (C.c_int, [_f, _f, _f, _vp, _vp, _vp]),
     "LBM_Strouhal": (_f, [_vp, C.c_int, C.c_int, C.c_int, _f, _f, _vp]),
+    "LBM_CdMonitorInit": (None, [_vp]),
+    "LBM_CdMonitorAdd": (C.c_int, [_vp, _f, _f]),
+    "LBM_TunnelCoefficients": (None, [_f, _f, _f, _f, _f, _f, _vp]),
+    "LBM_TunnelCdStartFrame": (C.c_int, [C.c_int, _f, C.c_int, C.c_int]),
+    "LBM_TunnelRampFactor": (_f, [C.c_int]),
+    "LBM_TunnelDefaults": (None, [_vp]),
+    "LBM_TunnelRun": (C.c_int, [_vp, _vp]),
 }
 
 _lib = None
@@ -447,3 +484,44 @@ def strouhal(cl_series, lbm_substeps: int, char_length: float, lattice_velocity:
     st = L.LBM_Strouhal(_p(cl), len(cl), lbm_substeps, sample_interval, char_length,
                         lattice_velocity, C.byref(f))
     return st, f.value
+
+
+class CdMonitor:
+    """The reference driver's Cd EMA / convergence monitor (LBM_CdMonitor*)."""
+
+    def __init__(self):
+        self._L = load()
+        self.m = LBMCdMonitor()
+        self._L.LBM_CdMonitorInit(C.byref(self.m))
+
+    def add(self, cd: float, cd_corr: float) -> bool:
+        return bool(self._L.LBM_CdMonitorAdd(C.byref(self.m), cd, cd_corr))
+
+
+def tunnel_coefficients(fx, fy, px, U, ref_area, blockage_factor) -> LBMCoefficients:
+    out = LBMCoefficients()
+    load().LBM_TunnelCoefficients(fx, fy, px, U, ref_area, blockage_factor, C.byref(out))
+    return out
+
+
+def tunnel_defaults() -> LBMTunnelOptions:
+    o = LBMTunnelOptions()
+    load().LBM_TunnelDefaults(C.byref(o))
+    return o
+
+
+def tunnel_run(**kw) -> LBMTunnelResult:
+    """Run the headless wind-tunnel loop (LBM_TunnelRun); keyword arguments
+    set LBMTunnelOptions fields (strings are encoded)."""
+    o = tunnel_defaults()
+    keep = []
+    for k, v in kw.items():
+        if isinstance(v, str):
+            v = os.fsencode(v)
+            keep.append(v)
+        setattr(o, k, v)
+    r = LBMTunnelResult()
+    rc = load().LBM_TunnelRun(C.byref(o), C.byref(r))
+    if rc != 0:
+        raise RuntimeError(f"LBM_TunnelRun failed: {load().LBM_GetErrorString(rc).decode()}")
+    return r

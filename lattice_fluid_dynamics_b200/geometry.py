@@ -127,3 +127,17 @@ def uv_sphere(radius: float, center=(0.0, 0.0, 0.0), n_theta: int = 32, n_phi: i
 def reynolds_tau(U: float, length_cells: float, Re: float) -> float:
     """tau = 3 nu + 1/2 with nu = U L / Re (simulation/src/main.c:447-448)."""
     return 3.0 * (U * length_cells / Re) + 0.5
+
+
+def write_obj(tris: np.ndarray, path: str) -> None:
+    """Write a triangle buffer (12 floats per triangle) as a Wavefront OBJ,
+    three vertices per face, printed with enough digits that every float32
+    coordinate reads back exactly."""
+    t = np.asarray(tris, np.float32).reshape(-1, 12)
+    with open(path, "w") as fh:
+        for row in t:
+            for k in range(3):
+                x, y, z = (float(v) for v in row[4 * k:4 * k + 3])
+                fh.write(f"v {x:.9g} {y:.9g} {z:.9g}\n")
+        for i in range(len(t)):
+            fh.write(f"f {3 * i + 1} {3 * i + 2} {3 * i + 3}\n")
