@@ -273,6 +273,43 @@ int LBM_ParticlesLoad(LBMParticles *p, const LBMParticle *host);
 void *LBM_ParticlesDevice(LBMParticles *p);
 
 /* ---------------------------------------------------------------------
+ * Batched sweeps: many independent grids advanced together, one kernel
+ * launch per lattice step for the whole batch (CUDA-graph replays of
+ * 32-step chunks), each grid with its own size, tau, operator,
+ * Smagorinsky constant, geometry, periodic flag and inlet velocity.  The
+ * reference runs one grid per process (main.c); a parameter sweep there is
+ * many processes.  Every grid's populations are bit-identical to stepping
+ * it alone with LBM_Step.
+ * ------------------------------------------------------------------- */
+typedef struct LBMBatch LBMBatch;
+
+/* Group `count` grids (caller-owned, all with the same storage format,
+ * LBM_ARITH_EXACT, already initialised).  The grids stay usable through the
+ * rest of the API between runs.  Returns NULL on invalid input. */
+LBMBatch *LBM_BatchCreate(LBMGrid **grids, int count);
+void LBM_BatchFree(LBMBatch *batch);
+
+/* Advance every grid by nSteps steps; inlet holds 3 floats per grid (the
+ * LBM_Step inlet velocity).  Asynchronous with respect to the host; later
+ * calls on any member grid are ordered after it.  Returns LBM_OK or an
+ * LBM_ERR_* code. */
+int LBM_BatchRun(LBMBatch *batch, int nSteps, const float *inlet);
+
+/* Choose each grid's tile width (32, 64, 128 or 256 cells along x; 256 /
+ * width rows) by timing `trialLaunches` launches of each candidate on that
+ * grid alone, writing into scratch memory (the grids' state is untouched).
+ * Returns LBM_OK or an LBM_ERR_* code. */
+int LBM_BatchAutotune(LBMBatch *batch, int trialLaunches);
+
+/* Tile shape of grid `index` (tileX cells along x by tileY rows). */
+int LBM_BatchGetTile(LBMBatch *batch, int index, int *tileX, int *tileY);
+int LBM_BatchSetTile(LBMBatch *batch, int index, int tileX);
+
+/* Thread blocks of one batched launch, and the CUDA stream of the batch. */
+long long LBM_BatchBlocksPerStep(LBMBatch *batch);
+void *LBM_BatchGetStream(LBMBatch *batch);
+
+/* ---------------------------------------------------------------------
  * Host side of the driver: OBJ ingestion, model placement, Re -> tau,
  * Strouhal number.  Plain C on the host, no device work.
  * ------------------------------------------------------------------- */

@@ -141,6 +141,14 @@ SIGNATURES = {
     "LBM_PlaceModel": (C.c_int, [_vp, _f, _vp, _vp, _vp]),
     "LBM_ReynoldsToTau": (C.c_int, [_f, _f, _f, _vp, _vp, _vp]),
     "LBM_Strouhal": (_f, [_vp, C.c_int, C.c_int, C.c_int, _f, _f, _vp]),
+    "LBM_BatchCreate": (_vp, [_vp, C.c_int]),
+    "LBM_BatchFree": (None, [_vp]),
+    "LBM_BatchRun": (C.c_int, [_vp, C.c_int, _vp]),
+    "LBM_BatchAutotune": (C.c_int, [_vp, C.c_int]),
+    "LBM_BatchGetTile": (C.c_int, [_vp, C.c_int, _vp, _vp]),
+    "LBM_BatchSetTile": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "LBM_BatchBlocksPerStep": (C.c_longlong, [_vp]),
+    "LBM_BatchGetStream": (_vp, [_vp]),
     "LBM_CdMonitorInit": (None, [_vp]),
     "LBM_CdMonitorAdd": (C.c_int, [_vp, _f, _f]),
     "LBM_TunnelCoefficients": (None, [_f, _f, _f, _f, _f, _f, _vp]),
@@ -525,3 +533,55 @@ def tunnel_run(**kw) -> LBMTunnelResult:
     if rc != 0:
         raise RuntimeError(f"LBM_TunnelRun failed: {load().LBM_GetErrorString(rc).decode()}")
     return r
+
+
+class Batch:
+    """Grids advanced together, one launch per step (LBM_Batch*)."""
+
+    def __init__(self, grids):
+        self._L = load()
+        self.grids = list(grids)
+        arr = (C.c_void_p * len(self.grids))(*[C.cast(g._g, C.c_void_p) for g in self.grids])
+        self._b = self._L.LBM_BatchCreate(arr, len(self.grids))
+        if not self._b:
+            raise RuntimeError("LBM_BatchCreate failed (uninitialised grid, mixed storage, "
+                               "fast arithmetic or a repeated grid)")
+
+    def close(self):
+        if getattr(self, "_b", None):
+            self._L.LBM_BatchFree(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, n: int, inlets):
+        inl = np.ascontiguousarray(inlets, np.float32).reshape(len(self.grids), 3)
+        rc = self._L.LBM_BatchRun(self._b, n, _p(inl))
+        if rc != 0:
+            raise RuntimeError(f"LBM_BatchRun: {self._L.LBM_GetErrorString(rc).decode()}")
+
+    def autotune(self, trial_launches: int = 10):
+        rc = self._L.LBM_BatchAutotune(self._b, trial_launches)
+        if rc != 0:
+            raise RuntimeError(f"LBM_BatchAutotune: {self._L.LBM_GetErrorString(rc).decode()}")
+
+    def tile(self, i: int):
+        tx, ty = C.c_int(), C.c_int()
+        assert self._L.LBM_BatchGetTile(self._b, i, C.byref(tx), C.byref(ty)) == 0
+        return tx.value, ty.value
+
+    def set_tile(self, i: int, tile_x: int):
+        if self._L.LBM_BatchSetTile(self._b, i, tile_x) != 0:
+            raise ValueError(f"tile width {tile_x}")
+
+    @property
+    def blocks_per_step(self) -> int:
+        return int(self._L.LBM_BatchBlocksPerStep(self._b))
+
+    @property
+    def stream(self) -> int:
+        return self._L.LBM_BatchGetStream(self._b) or 0

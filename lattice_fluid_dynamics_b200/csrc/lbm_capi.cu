@@ -223,6 +223,31 @@ bool sync(LBMGrid *grid) { return ok(grid, cudaStreamSynchronize(IMPL(grid)->str
 
 }  // namespace
 
+namespace lbm {
+StepArgs grid_step_args(LBMGrid *grid, float inX, float inY, float inZ) {
+    return step_args(grid, *IMPL(grid), inX, inY, inZ);
+}
+int grid_op(LBMGrid *grid) { return op_of(grid); }
+bool grid_enqueue_step(LBMGrid *grid, float inX, float inY, float inZ) {
+    return enqueue_step(grid, inX, inY, inZ);
+}
+bool grid_ok(LBMGrid *grid, cudaError_t e) { return ok(grid, e); }
+void grid_note_fused_steps(LBMGrid *grid, int k, float inX, float inY, float inZ) {
+    GridImpl &I = *IMPL(grid);
+    if (k <= 0) return;
+    // k fused steps from buffer gbuf: the last one read 1 - final gbuf
+    I.gbuf ^= (k & 1);
+    I.vin = 1 - I.gbuf;
+    I.vin_kind = IN_POST_COLLISION;
+    I.vin_periodic = I.stream_periodic;
+    I.vin_inlet[0] = inX;
+    I.vin_inlet[1] = inY;
+    I.vin_inlet[2] = inZ;
+    I.vel_valid = false;
+    I.stream_periodic = grid->periodicYZ;
+}
+}  // namespace lbm
+
 extern "C" {
 
 const char *LBM_GetErrorString(int code) {

@@ -26,6 +26,11 @@ cudaError_t launch_step(const GridImpl &g, const StepArgs &a, bool fused, int op
     LBM_DISPATCH(g.storage, step(g, a, fused, op, smag, s));
 }
 
+cudaError_t launch_step_batch(int storage, const BatchEntry *entries, const long long *starts,
+                              int count, long long blocks, int set, cudaStream_t s) {
+    LBM_DISPATCH(storage, batch(entries, starts, count, blocks, set, s));
+}
+
 static StepArgs stream_args(const GridImpl &g, const void *src, void *dst, int periodic) {
     StepArgs a{};
     a.src = src;

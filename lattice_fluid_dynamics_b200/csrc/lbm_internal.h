@@ -97,7 +97,39 @@ struct StepArgs {
     unsigned long long *guard;
 };
 
+// One grid of a batched step launch (k_step_batch): its step arguments,
+// operator, and tile shape -- 1 << lbx cells along x (32..256) by
+// 256 >> lbx rows, tiles_x * tiles_y tiles per z plane.
+struct BatchEntry {
+    StepArgs a;
+    int combo;    // op * 2 + smagorinsky
+    int lbx;
+    int tiles_x;
+    int tiles_y;
+};
+
+// Operator sets a batched kernel is compiled for: each single (op, smag)
+// combination, BGK + regularized, and all six.
+enum {
+    BATCH_SET_BGK = 0, BATCH_SET_BGK_SMAG, BATCH_SET_REG, BATCH_SET_REG_SMAG, BATCH_SET_MRT,
+    BATCH_SET_MRT_SMAG, BATCH_SET_BGK_REG, BATCH_SET_ALL
+};
+__host__ __device__ constexpr unsigned batch_set_mask(int set) {
+    return set < 6 ? (1u << set) : set == BATCH_SET_BGK_REG ? 0x5u : 0x3fu;
+}
+
+// lbm_capi.cu: the grid state machine, for the batched driver
+StepArgs grid_step_args(LBMGrid *grid, float inX, float inY, float inZ);
+int grid_op(LBMGrid *grid);
+bool grid_enqueue_step(LBMGrid *grid, float inX, float inY, float inZ);
+// the state transition of k fused steps run outside the grid's own launcher
+void grid_note_fused_steps(LBMGrid *grid, int k, float inX, float inY, float inZ);
+bool grid_ok(LBMGrid *grid, cudaError_t e);
+
 // lbm_step.cu
+cudaError_t launch_step_batch(int storage, const BatchEntry *entries_dev,
+                              const long long *starts_dev, int count, long long blocks, int set,
+                              cudaStream_t s);
 cudaError_t launch_step(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
                         bool fast_arith, cudaStream_t s);
 namespace fast {

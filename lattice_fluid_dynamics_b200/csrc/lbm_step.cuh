@@ -163,14 +163,13 @@ __device__ __forceinline__ int collide_cell(const StepArgs &a, typename S::R (&f
     return kind;
 }
 
-// The step.  CPT = cells per thread along x (1 or 2; 2 needs an even NX).
-template <class S, int OP, bool SMAG, bool FUSED, int CPT, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_step(const StepArgs a) {
+// One thread's share of a step: CPT cells starting at (x0, y, z).  CPT =
+// cells per thread along x (1 or 2; 2 needs an even NX).  `lane` is the
+// thread's lane in its warp (for the warp-aggregated guard count).
+template <class S, int OP, bool SMAG, bool FUSED, int CPT>
+__device__ __forceinline__ void step_cells(const StepArgs &a, int x0, int y, int z) {
     using T = typename S::T;
     using R = typename S::R;
-    const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * CPT;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z;
     if (x0 >= a.nx || y >= a.ny) return;
     const long long n = a.n;
     const long long cell0 =
@@ -242,8 +241,65 @@ __global__ void __launch_bounds__(256, MINB) k_step(const StepArgs a) {
     if (any) {
         int v = resets;
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(active, v, o);
-        if ((threadIdx.x & 31) == (unsigned)(__ffs(active) - 1) && v)
-            atomicAdd(a.guard, (unsigned long long)v);
+        const unsigned lane = (threadIdx.x + blockDim.x * threadIdx.y) & 31u;
+        if (lane == (unsigned)(__ffs(active) - 1) && v) atomicAdd(a.guard, (unsigned long long)v);
+    }
+}
+
+// The step over one grid: a 2D block tile of (bx * CPT) x by cells per z.
+template <class S, int OP, bool SMAG, bool FUSED, int CPT, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_step(const StepArgs a) {
+    step_cells<S, OP, SMAG, FUSED, CPT>(a, (blockIdx.x * blockDim.x + threadIdx.x) * CPT,
+                                        blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z);
+}
+
+// ---------------------------------------------------------------------------
+// Batched step: one launch advances every grid of a batch by one fused step.
+// The 1D grid of 256-thread blocks is the concatenation of each grid's
+// tiles; a block finds its grid by binary search over the tile offsets,
+// copies that grid's StepArgs into shared memory and runs the same per-cell
+// code as k_step, so every grid's result is bit-identical to a solo step.
+// Each grid has its own tile shape (BatchEntry::lbx).
+
+template <class S, int SET>
+__global__ void __launch_bounds__(256, 4) k_step_batch(const BatchEntry *__restrict__ entries,
+                                                        const long long *__restrict__ starts,
+                                                        int count) {
+    __shared__ BatchEntry e;
+    __shared__ int which;
+    if (threadIdx.x == 0) {
+        int lo = 0, hi = count - 1;  // largest i with starts[i] <= blockIdx.x
+        const long long b = blockIdx.x;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (starts[mid] <= b) lo = mid; else hi = mid - 1;
+        }
+        which = lo;
+    }
+    __syncthreads();
+    {
+        const int *src = reinterpret_cast<const int *>(entries + which);
+        int *dst = reinterpret_cast<int *>(&e);
+        for (int k = threadIdx.x; k < (int)(sizeof(BatchEntry) / sizeof(int)); k += blockDim.x)
+            dst[k] = src[k];
+    }
+    __syncthreads();
+    const long long local = (long long)blockIdx.x - starts[which];
+    const int tx = (int)(local % e.tiles_x);
+    const long long rest = local / e.tiles_x;
+    const int ty = (int)(rest % e.tiles_y);
+    const int z = (int)(rest / e.tiles_y);
+    const int bx = 1 << e.lbx;
+    const int x = tx * bx + (threadIdx.x & (bx - 1));
+    const int y = ty * (256 >> e.lbx) + (threadIdx.x >> e.lbx);
+    constexpr unsigned M = batch_set_mask(SET);
+    switch (e.combo) {
+        case 0: if constexpr ((M & 1u) != 0) step_cells<S, OP_BGK, false, true, 1>(e.a, x, y, z); break;
+        case 1: if constexpr ((M & 2u) != 0) step_cells<S, OP_BGK, true, true, 1>(e.a, x, y, z); break;
+        case 2: if constexpr ((M & 4u) != 0) step_cells<S, OP_REG, false, true, 1>(e.a, x, y, z); break;
+        case 3: if constexpr ((M & 8u) != 0) step_cells<S, OP_REG, true, true, 1>(e.a, x, y, z); break;
+        case 4: if constexpr ((M & 16u) != 0) step_cells<S, OP_MRT, false, true, 1>(e.a, x, y, z); break;
+        default: if constexpr ((M & 32u) != 0) step_cells<S, OP_MRT, true, true, 1>(e.a, x, y, z); break;
     }
 }
 
@@ -457,6 +513,23 @@ struct StepLaunch {
                                      cudaStream_t s) {
         k_mass_momentum<S><<<148 * 8, 256, 0, s>>>(static_cast<const typename S::T *>(f), g.n,
                                                    out4);
+        return cudaGetLastError();
+    }
+
+    static cudaError_t batch(const BatchEntry *entries, const long long *starts, int count,
+                             long long blocks, int set, cudaStream_t s) {
+        if (blocks <= 0 || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+        const unsigned nb = (unsigned)blocks;
+        switch (set) {
+            case BATCH_SET_BGK: k_step_batch<S, BATCH_SET_BGK><<<nb, 256, 0, s>>>(entries, starts, count); break;
+            case BATCH_SET_BGK_SMAG: k_step_batch<S, BATCH_SET_BGK_SMAG><<<nb, 256, 0, s>>>(entries, starts, count); break;
+            case BATCH_SET_REG: k_step_batch<S, BATCH_SET_REG><<<nb, 256, 0, s>>>(entries, starts, count); break;
+            case BATCH_SET_REG_SMAG: k_step_batch<S, BATCH_SET_REG_SMAG><<<nb, 256, 0, s>>>(entries, starts, count); break;
+            case BATCH_SET_MRT: k_step_batch<S, BATCH_SET_MRT><<<nb, 256, 0, s>>>(entries, starts, count); break;
+            case BATCH_SET_MRT_SMAG: k_step_batch<S, BATCH_SET_MRT_SMAG><<<nb, 256, 0, s>>>(entries, starts, count); break;
+            case BATCH_SET_BGK_REG: k_step_batch<S, BATCH_SET_BGK_REG><<<nb, 256, 0, s>>>(entries, starts, count); break;
+            default: k_step_batch<S, BATCH_SET_ALL><<<nb, 256, 0, s>>>(entries, starts, count); break;
+        }
         return cudaGetLastError();
     }
 };

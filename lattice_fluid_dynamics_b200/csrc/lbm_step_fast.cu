@@ -8,10 +8,6 @@
 namespace lbm {
 namespace fast {
 
-template struct StepLaunch<StoreF32>;
-template struct StepLaunch<StoreF16>;
-template struct StepLaunch<StoreBF16>;
-
 cudaError_t launch_step_fast(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
                              cudaStream_t s) {
     switch (g.storage) {

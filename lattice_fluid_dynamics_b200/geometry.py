@@ -12,7 +12,7 @@ r(theta, phi) around the centroid; the mesher samples that graph on a
 body is placed like simulation/src/main.c:289-349 places a model: scaled
 to the requested length and centred at world (-2, 0, 0).
 
-``sweep_shapes`` draws the uneven-size batched sweep of spheres,
+``sweep_instances`` draws the uneven-size batched sweep of spheres,
 ellipsoids and slanted boxes from a seed.
 """
 from __future__ import annotations
@@ -141,3 +141,103 @@ def write_obj(tris: np.ndarray, path: str) -> None:
                 fh.write(f"v {x:.9g} {y:.9g} {z:.9g}\n")
         for i in range(len(t)):
             fh.write(f"f {3 * i + 1} {3 * i + 2} {3 * i + 3}\n")
+
+
+def _cells_to_world(v: np.ndarray, dims) -> np.ndarray:
+    """Cell coordinates -> the reference's world coordinates: x = c / (NX/8) - 4,
+    y = c / (NY/4) - 2, z = c / (NZ/4) - 2 (simulation/src/lbm.c:353-362)."""
+    nx, ny, nz = dims
+    s = np.array([nx / 8.0, ny / 4.0, nz / 4.0])
+    return v / s - np.array([4.0, 2.0, 2.0])
+
+
+def _tris_from(verts: np.ndarray, faces) -> np.ndarray:
+    f = np.asarray(faces, np.int64)
+    out = np.zeros((len(f), 12), np.float32)
+    v = verts.astype(np.float32)
+    out[:, 0:3] = v[f[:, 0]]
+    out[:, 4:7] = v[f[:, 1]]
+    out[:, 8:11] = v[f[:, 2]]
+    return out
+
+
+def ellipsoid_cells(center, axes, n_theta: int = 24, n_phi: int = 24):
+    """Closed ellipsoid mesh in cell coordinates; `axes` are full lengths."""
+    th = np.linspace(0.0, math.pi, n_theta + 1)[1:-1]
+    ph = np.linspace(0.0, 2 * math.pi, n_phi, endpoint=False)
+    T, P = np.meshgrid(th, ph, indexing="ij")
+    d = np.stack([np.cos(T), np.sin(T) * np.cos(P), np.sin(T) * np.sin(P)], -1).reshape(-1, 3)
+    d = np.concatenate([d, [[1.0, 0, 0]], [[-1.0, 0, 0]]])
+    v = np.asarray(center) + 0.5 * np.asarray(axes) * d
+    nr = n_theta - 1
+    p0, p1 = nr * n_phi, nr * n_phi + 1
+    faces = []
+    for j in range(n_phi):
+        jn = (j + 1) % n_phi
+        faces.append((p0, jn, j))
+        faces.append((p1, (nr - 1) * n_phi + j, (nr - 1) * n_phi + jn))
+    for i in range(nr - 1):
+        for j in range(n_phi):
+            jn = (j + 1) % n_phi
+            a, b, c, e = i * n_phi + j, i * n_phi + jn, (i + 1) * n_phi + j, (i + 1) * n_phi + jn
+            faces.append((a, b, e))
+            faces.append((a, e, c))
+    return v, faces
+
+
+def slanted_box_cells(center, size, slant_deg: float):
+    """Box of `size` (L, W, H) cells whose rear top edge is lowered by a slant
+    of `slant_deg` over the rear half of its length; 12 triangles."""
+    L, W, H = size
+    cx, cy, cz = center
+    x0, x1 = cx - L / 2, cx + L / 2
+    y0, y1 = cy - W / 2, cy + W / 2
+    z0, z1 = cz - H / 2, cz + H / 2
+    drop = min(0.5 * L * math.tan(math.radians(slant_deg)), 0.8 * H)
+    v = np.array([[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0],
+                  [x0, y0, z1], [x1, y0, z1 - drop], [x1, y1, z1 - drop], [x0, y1, z1]])
+    quads = [(0, 3, 2, 1), (4, 5, 6, 7), (0, 1, 5, 4), (2, 3, 7, 6), (1, 2, 6, 5), (0, 4, 7, 3)]
+    faces = []
+    for a, b, c, d in quads:
+        faces += [(a, b, c), (a, c, d)]
+    return v, faces
+
+
+def sweep_instances(seed: int = 1, count: int = 64):
+    """The batched parameter sweep: `count` instances drawn from `seed`.
+
+    Grid sizes uniform between 64^3 and 192x96x96 (multiples of 8); one body
+    per grid -- a sphere, an ellipsoid (axes 6-20 cells) or a slanted box
+    (sides 6-20 cells, slant 15-35 degrees) -- centred at 30 % of the length
+    and mid-height; U ~ U[0.02, 0.10], Re ~ U[100, 2000] with the body length
+    in cells as the length scale; BGK or regularized collision; periodic
+    y/z.  Each instance is a dict with dims, kind, triangles (world
+    coordinates) and bbox, U, Re, length, op ("bgk" | "reg")."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        nx = 64 + 8 * int(rng.integers(0, 17))
+        ny = 64 + 8 * int(rng.integers(0, 5))
+        nz = 64 + 8 * int(rng.integers(0, 5))
+        kind = ("sphere", "ellipsoid", "slanted_box")[int(rng.integers(0, 3))]
+        c = (0.3 * nx, 0.5 * ny, 0.5 * nz)
+        if kind == "sphere":
+            d = float(rng.uniform(6, 20))
+            axes = (d, d, d)
+            v, f = ellipsoid_cells(c, axes)
+        elif kind == "ellipsoid":
+            axes = tuple(float(a) for a in rng.uniform(6, 20, 3))
+            v, f = ellipsoid_cells(c, axes)
+        else:
+            axes = tuple(float(a) for a in rng.uniform(6, 20, 3))
+            v, f = slanted_box_cells(c, axes, float(rng.uniform(15, 35)))
+        w = _cells_to_world(v, (nx, ny, nz))
+        tris = _tris_from(w, f)
+        lo, hi = w.min(0), w.max(0)
+        bbox = tuple(float(x) for x in (*lo, *hi))
+        U = float(rng.uniform(0.02, 0.10))
+        Re = float(rng.uniform(100, 2000))
+        op = "bgk" if rng.integers(0, 2) == 0 else "reg"
+        out.append(dict(index=k, dims=(nx, ny, nz), kind=kind, axes=axes, triangles=tris,
+                        bbox=bbox, U=U, Re=Re, length=float(axes[0]), op=op))
+    return out

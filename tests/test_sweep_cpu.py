@@ -1,0 +1,46 @@
+"""The batched-sweep instance generator (host only)."""
+from __future__ import annotations
+
+from collections import Counter
+
+import numpy as np
+
+from lattice_fluid_dynamics_b200 import geometry
+
+
+def _closed(tris: np.ndarray) -> bool:
+    """Every edge of a closed triangle mesh is shared by exactly two faces."""
+    edges = Counter()
+    v = tris.reshape(-1, 3, 4)[:, :, :3]
+    for t in v:
+        for a, b in ((0, 1), (1, 2), (2, 0)):
+            e = tuple(sorted((tuple(t[a]), tuple(t[b]))))
+            edges[e] += 1
+    return all(c == 2 for c in edges.values())
+
+
+def test_sweep_instances_deterministic_and_in_range():
+    a = geometry.sweep_instances(1, 64)
+    b = geometry.sweep_instances(1, 64)
+    assert len(a) == 64
+    for x, y in zip(a, b):
+        assert x["dims"] == y["dims"] and np.array_equal(x["triangles"], y["triangles"])
+    for i in a:
+        nx, ny, nz = i["dims"]
+        assert 64 <= nx <= 192 and 64 <= ny <= 96 and 64 <= nz <= 96
+        assert nx % 8 == ny % 8 == nz % 8 == 0
+        assert 0.02 <= i["U"] <= 0.10 and 100 <= i["Re"] <= 2000
+        assert all(6 <= ax <= 20 for ax in i["axes"])
+        assert i["op"] in ("bgk", "reg") and i["kind"] in ("sphere", "ellipsoid", "slanted_box")
+        lo = np.array(i["bbox"][:3])
+        hi = np.array(i["bbox"][3:])
+        assert np.all(lo > [-4, -2, -2]) and np.all(hi < [4, 2, 2])
+    kinds = Counter(i["kind"] for i in a)
+    assert len(kinds) == 3
+    assert geometry.sweep_instances(2, 4)[0]["dims"] != a[0]["dims"] or \
+        not np.array_equal(geometry.sweep_instances(2, 4)[0]["triangles"], a[0]["triangles"])
+
+
+def test_sweep_meshes_closed():
+    for i in geometry.sweep_instances(1, 12):
+        assert _closed(i["triangles"]), i["kind"]
