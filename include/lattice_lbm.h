@@ -305,8 +305,10 @@ int LBM_BatchAutotune(LBMBatch *batch, int trialLaunches);
 int LBM_BatchGetTile(LBMBatch *batch, int index, int *tileX, int *tileY);
 int LBM_BatchSetTile(LBMBatch *batch, int index, int tileX);
 
-/* Thread blocks of one batched launch, and the CUDA stream of the batch. */
-long long LBM_BatchBlocksPerStep(LBMBatch *batch);
+/* 256-cell tiles of one batched step (all grids), and the CUDA stream of
+ * the batch.  A launch runs a fixed number of persistent blocks (a few per
+ * SM) that stride over the tiles. */
+long long LBM_BatchTilesPerStep(LBMBatch *batch);
 void *LBM_BatchGetStream(LBMBatch *batch);
 
 /* ---------------------------------------------------------------------

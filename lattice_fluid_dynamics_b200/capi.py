@@ -147,7 +147,7 @@ SIGNATURES = {
     "LBM_BatchAutotune": (C.c_int, [_vp, C.c_int]),
     "LBM_BatchGetTile": (C.c_int, [_vp, C.c_int, _vp, _vp]),
     "LBM_BatchSetTile": (C.c_int, [_vp, C.c_int, C.c_int]),
-    "LBM_BatchBlocksPerStep": (C.c_longlong, [_vp]),
+    "LBM_BatchTilesPerStep": (C.c_longlong, [_vp]),
     "LBM_BatchGetStream": (_vp, [_vp]),
     "LBM_CdMonitorInit": (None, [_vp]),
     "LBM_CdMonitorAdd": (C.c_int, [_vp, _f, _f]),
@@ -579,8 +579,8 @@ class Batch:
             raise ValueError(f"tile width {tile_x}")
 
     @property
-    def blocks_per_step(self) -> int:
-        return int(self._L.LBM_BatchBlocksPerStep(self._b))
+    def tiles_per_step(self) -> int:
+        return int(self._L.LBM_BatchTilesPerStep(self._b))
 
     @property
     def stream(self) -> int:

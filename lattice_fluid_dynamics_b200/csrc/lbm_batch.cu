@@ -1,7 +1,8 @@
 // Batched sweeps (LBM_Batch*): one kernel launch per lattice step advances
 // every grid of a batch.
 //
-// Each launch is k_step_batch over the concatenated tiles of all grids; the
+// Each launch is k_step_batch over the concatenated tiles of all grids (a
+// persistent launch of a few blocks per SM striding over the tiles); the
 // per-grid arguments live in device memory (two arrays, one per buffer
 // parity, since consecutive steps swap source and destination), so a CUDA
 // graph of a 32-step chunk (A, B, A, B, ...) is independent of the
@@ -13,6 +14,7 @@
 // geometry edit) first take their priming steps through their own
 // launcher; every grid takes the same number of such steps so that the
 // batch stays in lock step.
+#include <stdlib.h>
 #include <string.h>
 
 #include <new>
@@ -39,8 +41,10 @@ struct LBMBatch {
     cudaEvent_t copied[2] = {nullptr, nullptr};
     bool copy_pending[2] = {false, false};
     int runs = 0;
-    long long blocks = 0;
+    long long blocks = 0;                 // tiles of one step (all grids)
     int set = BATCH_SET_ALL;
+    int minb = 4;                         // resident blocks per SM the kernel is built for
+    unsigned persist = 0;                 // persistent blocks of a full launch
     cudaGraphExec_t graph = nullptr;
     long long graph_blocks = -1;
     int graph_set = -1;
@@ -86,6 +90,10 @@ void drop_graph(LBMBatch &b) {
 
 bool fail(LBMGrid *any, cudaError_t e) { return !grid_ok(any, e); }
 
+unsigned persist_blocks(const LBMBatch &b) {
+    return (unsigned)(b.blocks < (long long)b.persist ? b.blocks : (long long)b.persist);
+}
+
 }  // namespace
 
 extern "C" {
@@ -109,6 +117,18 @@ LBMBatch *LBM_BatchCreate(LBMGrid **grids, int count) {
     b->grids.assign(grids, grids + count);
     b->lbx.assign(count, 5);  // 32 x 8 tiles, the single-grid default
     b->grid_done.assign(count, nullptr);
+    // persistent launch: minb blocks per SM (LBM_BATCH_MINB=3 trades
+    // occupancy for registers)
+    const char *menv = getenv("LBM_BATCH_MINB");
+    b->minb = (menv && atoi(menv) == 3) ? 3 : 4;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        sms <= 0) {
+        delete b;
+        return nullptr;
+    }
+    b->persist = (unsigned)(sms * b->minb);
     bool good = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess;
     good = good && cudaEventCreateWithFlags(&b->batch_done, cudaEventDisableTiming) == cudaSuccess;
     for (int i = 0; good && i < count; i++)
@@ -220,7 +240,8 @@ int LBM_BatchRun(LBMBatch *b, int nSteps, const float *inlet) {
                                                          cudaStreamCaptureModeThreadLocal));
             for (int k = 0; good && k < kChunk; k++)
                 good = !fail(g0, launch_step_batch(b->storage, (k & 1) ? eb : ea, b->starts_dev,
-                                                   n, total, b->set, b->stream));
+                                                   n, total, b->set, b->minb, persist_blocks(*b),
+                                                   b->stream));
             const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
             good = good && !fail(g0, e);
             cudaGraphExec_t exec = nullptr;
@@ -238,7 +259,7 @@ int LBM_BatchRun(LBMBatch *b, int nSteps, const float *inlet) {
     }
     for (int k = 0; k < left; k++)
         if (fail(g0, launch_step_batch(b->storage, (k & 1) ? eb : ea, b->starts_dev, n, total,
-                                       b->set, b->stream)))
+                                       b->set, b->minb, persist_blocks(*b), b->stream)))
             return LBM_ERR_CUDA;
 
     // every grid's later work waits for the batch
@@ -293,12 +314,14 @@ int LBM_BatchAutotune(LBMBatch *b, int trialLaunches) {
                                             b->stream)) &&
                    !fail(g, cudaStreamSynchronize(b->stream));
             // one untimed launch, then the timed ones
+            const unsigned pb = (unsigned)(starts[1] < (long long)b->persist ? starts[1]
+                                                                               : b->persist);
             good = good && !fail(g, launch_step_batch(b->storage, ent, st, 1, starts[1], set,
-                                                      b->stream));
+                                                      b->minb, pb, b->stream));
             good = good && !fail(g, cudaEventRecord(t0, b->stream));
             for (int k = 0; good && k < trialLaunches; k++)
                 good = !fail(g, launch_step_batch(b->storage, ent, st, 1, starts[1], set,
-                                                  b->stream));
+                                                  b->minb, pb, b->stream));
             good = good && !fail(g, cudaEventRecord(t1, b->stream)) &&
                    !fail(g, cudaEventSynchronize(t1));
             float ms = 0;
@@ -342,7 +365,7 @@ int LBM_BatchSetTile(LBMBatch *b, int index, int tileX) {
     return LBM_OK;
 }
 
-long long LBM_BatchBlocksPerStep(LBMBatch *b) {
+long long LBM_BatchTilesPerStep(LBMBatch *b) {
     if (!b) return 0;
     long long total = 0;
     for (int i = 0; i < b->count; i++) {

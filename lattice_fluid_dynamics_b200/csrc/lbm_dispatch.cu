@@ -27,8 +27,9 @@ cudaError_t launch_step(const GridImpl &g, const StepArgs &a, bool fused, int op
 }
 
 cudaError_t launch_step_batch(int storage, const BatchEntry *entries, const long long *starts,
-                              int count, long long blocks, int set, cudaStream_t s) {
-    LBM_DISPATCH(storage, batch(entries, starts, count, blocks, set, s));
+                              int count, long long tiles, int set, int minb, unsigned blocks,
+                              cudaStream_t s) {
+    LBM_DISPATCH(storage, batch(entries, starts, count, tiles, set, minb, blocks, s));
 }
 
 static StepArgs stream_args(const GridImpl &g, const void *src, void *dst, int periodic) {

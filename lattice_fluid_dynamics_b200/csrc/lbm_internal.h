@@ -127,9 +127,11 @@ void grid_note_fused_steps(LBMGrid *grid, int k, float inX, float inY, float inZ
 bool grid_ok(LBMGrid *grid, cudaError_t e);
 
 // lbm_step.cu
+// `tiles` tiles of all grids processed by `blocks` persistent blocks, the
+// kernel built for at least `minb` (3 or 4) resident blocks per SM
 cudaError_t launch_step_batch(int storage, const BatchEntry *entries_dev,
-                              const long long *starts_dev, int count, long long blocks, int set,
-                              cudaStream_t s);
+                              const long long *starts_dev, int count, long long tiles, int set,
+                              int minb, unsigned blocks, cudaStream_t s);
 cudaError_t launch_step(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
                         bool fast_arith, cudaStream_t s);
 namespace fast {
