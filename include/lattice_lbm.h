@@ -312,6 +312,51 @@ long long LBM_BatchTilesPerStep(LBMBatch *batch);
 void *LBM_BatchGetStream(LBMBatch *batch);
 
 /* ---------------------------------------------------------------------
+ * Warm-start network kernels (no counterpart in the reference, whose
+ * learned components are CPU MLPs).  3x3x3 convolutions with zero padding
+ * over channels-last BF16 activations on the tensor cores (tcgen05, FP32
+ * accumulation).  All pointers are device pointers; channel counts,
+ * strides and offsets are multiples of 8.  Weights are BF16
+ * [coutPad][LBM_NNKPad(cin)] with k = tap * cin + c, tap = (dz+1)*9 +
+ * (dy+1)*3 + (dx+1), zero-padded.  coutPad is 16, 32, 48, 64, 96, 128 or
+ * 192 (forward) and 16, 32, 64 or 128 (weight gradient).  Calls are
+ * asynchronous on `stream` (a cudaStream_t).
+ * ------------------------------------------------------------------- */
+
+/* 27 * cin rounded up to a multiple of 128. */
+int LBM_NNKPad(int cin);
+
+/* y = act(conv(x, w) + bias) for the first coutStore output channels;
+ * act 0 = linear, 1 = leaky ReLU (slope 0.1).  Output to BF16 `y` and/or
+ * FP32 `y32` (both with stride yStride and offset yOff; `accumulate` adds
+ * into y32).  The input gradient of a convolution is this call on the
+ * weights from LBM_NNWeightTranspose with act = 0. */
+int LBM_NNConvForward(const void *x, int xStride, int xOff, int cin, const void *w,
+                      const float *bias, int coutPad, int act, void *y, float *y32, int yStride,
+                      int yOff, int coutStore, int accumulate, int nb, int nz, int ny, int nx,
+                      void *stream);
+
+/* wt[ci][(26 - tap) * cout + co] = w[co][tap * cin + ci]: the weights of
+ * the input-gradient convolution, [wtRows][LBM_NNKPad(cout)], rows >= cin
+ * zero. */
+int LBM_NNWeightTranspose(const void *w, int cout, int cin, void *wt, int wtRows, void *stream);
+
+/* dw[co][k] (+)= sum over voxels of g[v][co] * x[neighbour(v, tap)][c],
+ * k = tap * cin + c < 27 * cin, co < cout; FP32 result.  The reduction
+ * runs over chunksPerSplit * 64 voxels per CTA with FP32 partial tiles in
+ * `workspace` (LBM_NNWgradWorkspaceBytes) summed in a fixed order. */
+long long LBM_NNWgradWorkspaceBytes(int cin, int coutPad, int nb, int nz, int ny, int nx,
+                                    int chunksPerSplit);
+int LBM_NNConvWeightGrad(const void *x, int xStride, int xOff, int cin, const void *g,
+                         int gStride, int cout, int coutPad, float *dw, int accumulate,
+                         float *workspace, long long workspaceBytes, int chunksPerSplit, int nb,
+                         int nz, int ny, int nx, void *stream);
+
+/* Synchronises the device; LBM_ERR_TIMEOUT if a convolution kernel gave up
+ * waiting for its tensor-core work since the last call, else LBM_OK. */
+int LBM_NNTakeError(void);
+
+/* ---------------------------------------------------------------------
  * Host side of the driver: OBJ ingestion, model placement, Re -> tau,
  * Strouhal number.  Plain C on the host, no device work.
  * ------------------------------------------------------------------- */

@@ -149,6 +149,16 @@ SIGNATURES = {
     "LBM_BatchSetTile": (C.c_int, [_vp, C.c_int, C.c_int]),
     "LBM_BatchTilesPerStep": (C.c_longlong, [_vp]),
     "LBM_BatchGetStream": (_vp, [_vp]),
+    "LBM_NNKPad": (C.c_int, [C.c_int]),
+    "LBM_NNConvForward": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, C.c_int,
+                                    _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                    C.c_int, C.c_int, C.c_int, _vp]),
+    "LBM_NNWeightTranspose": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp]),
+    "LBM_NNWgradWorkspaceBytes": (C.c_longlong, [C.c_int] * 7),
+    "LBM_NNConvWeightGrad": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, C.c_int,
+                                       C.c_int, _vp, C.c_int, _vp, C.c_longlong, C.c_int,
+                                       C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
+    "LBM_NNTakeError": (C.c_int, []),
     "LBM_CdMonitorInit": (None, [_vp]),
     "LBM_CdMonitorAdd": (C.c_int, [_vp, _f, _f]),
     "LBM_TunnelCoefficients": (None, [_f, _f, _f, _f, _f, _f, _vp]),

@@ -1,0 +1,25 @@
+// Launchers of the warm-start network's convolution kernels (lbm_nn.cu),
+// shared with the network driver.  Not part of the public ABI.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace lbm {
+namespace nn {
+
+struct ConvFwdArgs;
+struct ConvWgradArgs;
+
+// K (27 taps x cin) rounded up to a multiple of 128
+int k_pad_of(int cin);
+cudaError_t conv_forward(const ConvFwdArgs &a, int nt, cudaStream_t s);
+cudaError_t conv_wgrad(const ConvWgradArgs &a, int nt, unsigned splits, float *dw, int accumulate,
+                       cudaStream_t s);
+cudaError_t weight_transpose(const __nv_bfloat16 *w, int cout, int cin, __nv_bfloat16 *wt,
+                             int wt_rows, cudaStream_t s);
+// reads and clears the device error word of the GEMM kernels (synchronous)
+int take_error();
+
+}  // namespace nn
+}  // namespace lbm
