@@ -356,6 +356,49 @@ int LBM_NNConvWeightGrad(const void *x, int xStride, int xOff, int cin, const vo
  * waiting for its tensor-core work since the last call, else LBM_OK. */
 int LBM_NNTakeError(void);
 
+/* The warm-start network: a 4-level 3D conv encoder-decoder (8->16->32->64
+ * ->128 channels and back, skip connections, ~1.9 M parameters, leaky ReLU)
+ * mapping per-voxel (solid fraction, U, Re) at 1/4 of the grid's resolution
+ * to ((rho - 1) / U^2, u / U).  BF16 activations and weights, FP32 master
+ * weights, Adam; forward and backward run on the kernels above.  nx, ny, nz
+ * are the network's resolution (multiples of 8); features are float
+ * [batch][voxel][3] = (solid fraction, U, Re), targets and predictions
+ * float [batch][voxel][4].  Parameters are packed layer by layer as
+ * (w [cout][27 cin], b [cout]).  The *Device variants take device
+ * pointers; the others host pointers.  All synchronise the network's
+ * stream and return LBM_OK or an LBM_ERR_* code. */
+typedef struct LBMWarmNet LBMWarmNet;
+long long LBM_WarmNetParamCount(void);
+LBMWarmNet *LBM_WarmNetCreate(int nx, int ny, int nz, int maxBatch, unsigned seed);
+void LBM_WarmNetFree(LBMWarmNet *net);
+int LBM_WarmNetGetParams(LBMWarmNet *net, float *host);
+int LBM_WarmNetSetParams(LBMWarmNet *net, const float *host);
+int LBM_WarmNetForward(LBMWarmNet *net, const float *features, int batch, float *pred);
+int LBM_WarmNetForwardDevice(LBMWarmNet *net, const float *features, int batch, float *pred);
+/* mean squared error and (gradHost != NULL) its gradient, packed like the
+ * parameters */
+int LBM_WarmNetLossGrad(LBMWarmNet *net, const float *features, const float *target, int batch,
+                        double *loss, float *gradHost);
+int LBM_WarmNetLossGradDevice(LBMWarmNet *net, const float *features, const float *target,
+                              int batch, double *loss, float *gradHost);
+/* one Adam step (beta 0.9 / 0.999) at learning rate lr; *loss before it */
+int LBM_WarmNetTrainStep(LBMWarmNet *net, const float *features, const float *target, int batch,
+                         float lr, double *loss);
+int LBM_WarmNetTrainStepDevice(LBMWarmNet *net, const float *features, const float *target,
+                               int batch, float lr, double *loss);
+void *LBM_WarmNetGetStream(LBMWarmNet *net);
+/* Features / targets of a grid at 1/factor resolution into device arrays:
+ * solid fraction of each factor^3 block with U and Re; block means of
+ * ((rho - 1) / U^2, u / U) over fluid cells (solid cells count as rho = 1,
+ * u = 0) of the grid's current velocity field. */
+int LBM_WarmNetGridFeatures(LBMGrid *grid, int factor, float U, float Re, float *featDev);
+int LBM_WarmNetGridTargets(LBMGrid *grid, int factor, float U, float *targetDev);
+/* Warm start: run the network on the grid's mask (grid = factor x network
+ * resolution on every axis), interpolate its prediction trilinearly to the
+ * grid, and initialise f = f_new = feq(rho, u) (solid cells rho = 1, u = 0)
+ * -- LBM_InitializeFlow with a predicted field instead of a uniform one. */
+int LBM_InitializeFromWarmNet(LBMGrid *grid, LBMWarmNet *net, float U, float Re);
+
 /* ---------------------------------------------------------------------
  * Host side of the driver: OBJ ingestion, model placement, Re -> tau,
  * Strouhal number.  Plain C on the host, no device work.

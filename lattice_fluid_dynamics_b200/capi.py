@@ -159,6 +159,21 @@ SIGNATURES = {
                                        C.c_int, _vp, C.c_int, _vp, C.c_longlong, C.c_int,
                                        C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
     "LBM_NNTakeError": (C.c_int, []),
+    "LBM_WarmNetParamCount": (C.c_longlong, []),
+    "LBM_WarmNetCreate": (_vp, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint]),
+    "LBM_WarmNetFree": (None, [_vp]),
+    "LBM_WarmNetGetParams": (C.c_int, [_vp, _vp]),
+    "LBM_WarmNetSetParams": (C.c_int, [_vp, _vp]),
+    "LBM_WarmNetForward": (C.c_int, [_vp, _vp, C.c_int, _vp]),
+    "LBM_WarmNetForwardDevice": (C.c_int, [_vp, _vp, C.c_int, _vp]),
+    "LBM_WarmNetLossGrad": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp]),
+    "LBM_WarmNetLossGradDevice": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp]),
+    "LBM_WarmNetTrainStep": (C.c_int, [_vp, _vp, _vp, C.c_int, _f, _vp]),
+    "LBM_WarmNetTrainStepDevice": (C.c_int, [_vp, _vp, _vp, C.c_int, _f, _vp]),
+    "LBM_WarmNetGetStream": (_vp, [_vp]),
+    "LBM_WarmNetGridFeatures": (C.c_int, [_G, C.c_int, _f, _f, _vp]),
+    "LBM_WarmNetGridTargets": (C.c_int, [_G, C.c_int, _f, _vp]),
+    "LBM_InitializeFromWarmNet": (C.c_int, [_G, _vp, _f, _f]),
     "LBM_CdMonitorInit": (None, [_vp]),
     "LBM_CdMonitorAdd": (C.c_int, [_vp, _f, _f]),
     "LBM_TunnelCoefficients": (None, [_f, _f, _f, _f, _f, _f, _vp]),
@@ -595,3 +610,81 @@ class Batch:
     @property
     def stream(self) -> int:
         return self._L.LBM_BatchGetStream(self._b) or 0
+
+
+class WarmNet:
+    """The warm-start network (LBM_WarmNet*); arrays are numpy float32."""
+
+    def __init__(self, nx: int, ny: int, nz: int, max_batch: int = 1, seed: int = 0):
+        self._L = load()
+        self._n = self._L.LBM_WarmNetCreate(nx, ny, nz, max_batch, seed)
+        if not self._n:
+            raise RuntimeError("LBM_WarmNetCreate failed")
+        self.dims = (nz, ny, nx)
+        self.vox = nx * ny * nz
+        self.max_batch = max_batch
+
+    def close(self):
+        if getattr(self, "_n", None):
+            self._L.LBM_WarmNetFree(self._n)
+            self._n = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._n
+
+    @staticmethod
+    def param_count() -> int:
+        return int(load().LBM_WarmNetParamCount())
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what}: {self._L.LBM_GetErrorString(rc).decode()}")
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.param_count(), np.float32)
+        self._check(self._L.LBM_WarmNetGetParams(self._n, _p(out)), "LBM_WarmNetGetParams")
+        return out
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.param_count()
+        self._check(self._L.LBM_WarmNetSetParams(self._n, _p(p)), "LBM_WarmNetSetParams")
+
+    def forward(self, features: np.ndarray) -> np.ndarray:
+        f = np.ascontiguousarray(features, np.float32)
+        b = f.size // (3 * self.vox)
+        out = np.empty((b, self.vox, 4), np.float32)
+        self._check(self._L.LBM_WarmNetForward(self._n, _p(f), b, _p(out)), "forward")
+        return out
+
+    def loss_grad(self, features, target, want_grad=True):
+        f = np.ascontiguousarray(features, np.float32)
+        t = np.ascontiguousarray(target, np.float32)
+        b = f.size // (3 * self.vox)
+        loss = C.c_double()
+        g = np.empty(self.param_count(), np.float32) if want_grad else None
+        self._check(self._L.LBM_WarmNetLossGrad(self._n, _p(f), _p(t), b, C.byref(loss),
+                                                None if g is None else _p(g)), "loss_grad")
+        return loss.value, g
+
+    def train_step(self, features, target, lr: float) -> float:
+        f = np.ascontiguousarray(features, np.float32)
+        t = np.ascontiguousarray(target, np.float32)
+        b = f.size // (3 * self.vox)
+        loss = C.c_double()
+        self._check(self._L.LBM_WarmNetTrainStep(self._n, _p(f), _p(t), b, lr, C.byref(loss)),
+                    "train_step")
+        return loss.value
+
+    def train_step_device(self, feat_ptr: int, target_ptr: int, batch: int, lr: float) -> float:
+        loss = C.c_double()
+        self._check(self._L.LBM_WarmNetTrainStepDevice(self._n, feat_ptr, target_ptr, batch, lr,
+                                                       C.byref(loss)), "train_step_device")
+        return loss.value

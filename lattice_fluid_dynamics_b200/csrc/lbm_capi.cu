@@ -465,6 +465,34 @@ int LBM_InitializeFlow(LBMGrid *grid, float ux, float uy, float uz) {
     return 1;
 }
 
+}  // extern "C"
+
+namespace lbm {
+// f = f_new = feq(rho, u) from device fields; the state machine restarts
+// from an explicit f (shared by LBM_InitializeFromField and the warm start)
+int grid_init_from_device(LBMGrid *grid, const float *drho, const float *du) {
+    GridImpl *I = IMPL(grid);
+    drop_graph(*I);
+    bool good = ok(grid, launch_init_field(*I, I->pop[0], I->pop[1], drho, du, I->stream));
+    if (good) {
+        k_vel_from_field<<<(unsigned)((I->n + 255) / 256), 256, 0, I->stream>>>(
+            I->vel, I->vel64, I->n, drho, du);
+        good = ok(grid, cudaGetLastError());
+    }
+    good = good && ok(grid, cudaMemsetAsync(I->guard, 0, sizeof(unsigned long long), I->stream));
+    good = good && sync(grid);
+    if (!good) return 0;
+    I->fbuf = 0;
+    I->gbuf = 1;
+    I->vel_valid = true;
+    I->stream_periodic = grid->periodicYZ;
+    I->initialized = true;
+    return 1;
+}
+}  // namespace lbm
+
+extern "C" {
+
 int LBM_InitializeFromField(LBMGrid *grid, const float *rho, const float *u) {
     GridImpl *I = IMPL(grid);
     if (!I || !rho || !u) {
@@ -480,22 +508,10 @@ int LBM_InitializeFromField(LBMGrid *grid, const float *rho, const float *u) {
                                     I->stream));
     good = good && ok(grid, cudaMemcpyAsync(du, u, sizeof(float) * 3 * (size_t)I->n,
                                             cudaMemcpyHostToDevice, I->stream));
-    good = good && ok(grid, launch_init_field(*I, I->pop[0], I->pop[1], drho, du, I->stream));
-    if (good) {
-        k_vel_from_field<<<(unsigned)((I->n + 255) / 256), 256, 0, I->stream>>>(
-            I->vel, I->vel64, I->n, drho, du);
-        good = ok(grid, cudaGetLastError());
-    }
-    good = good && ok(grid, cudaMemsetAsync(I->guard, 0, sizeof(unsigned long long), I->stream));
+    const int r = good ? grid_init_from_device(grid, drho, du) : 0;
     cudaFreeAsync(d, I->stream);
-    good = good && sync(grid);
-    if (!good) return 0;
-    I->fbuf = 0;
-    I->gbuf = 1;
-    I->vel_valid = true;
-    I->stream_periodic = grid->periodicYZ;
-    I->initialized = true;
-    return 1;
+    sync(grid);
+    return r;
 }
 
 void LBM_Step(LBMGrid *grid, float inletVelX, float inletVelY, float inletVelZ) {

@@ -28,9 +28,12 @@ cudaError_t set_attr(int slot) {
     if (g_attr_done[slot]) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(k_conv_fwd<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          gemm_smem_bytes<NT>());
-    if (e == cudaSuccess && (NT == 16 || NT == 32 || NT == 64 || NT == 128))
-        e = cudaFuncSetAttribute(k_conv_wgrad<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 gemm_smem_bytes<NT>());
+    if constexpr (NT == 16 || NT == 32 || NT == 64 || NT == 128) {
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_conv_wgrad<NT>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     gemm_smem_bytes<NT>());
+    }
     if (e == cudaSuccess) g_attr_done[slot] = true;
     return e;
 }
@@ -58,6 +61,7 @@ cudaError_t fwd_nt(ConvFwdArgs a, int slot, cudaStream_t s) {
 
 template <int NT>
 cudaError_t wgrad_nt(ConvWgradArgs a, int slot, unsigned splits, cudaStream_t s) {
+    static_assert(NT == 16 || NT == 32 || NT == 64 || NT == 128, "weight-gradient tile");
     cudaError_t e = set_attr<NT>(slot);
     if (e != cudaSuccess) return e;
     k_conv_wgrad<NT><<<dim3(a.k_pad / 128, splits), 128, gemm_smem_bytes<NT>(), s>>>(a);
@@ -109,7 +113,7 @@ cudaError_t conv_forward(const ConvFwdArgs &a0, int nt, cudaStream_t s) {
 }
 
 cudaError_t conv_wgrad(const ConvWgradArgs &a0, int nt, unsigned splits, float *dw,
-                       int accumulate, cudaStream_t s) {
+                       int accumulate, cudaStream_t s, int cout_write) {
     ConvWgradArgs a = a0;
     a.err = err_ptr();
     if (!a.err) return cudaErrorInvalidDevicePointer;
@@ -122,9 +126,10 @@ cudaError_t conv_wgrad(const ConvWgradArgs &a0, int nt, unsigned splits, float *
         default: return cudaErrorInvalidValue;
     }
     if (e != cudaSuccess) return e;
-    const int total = a.cout * a.k_real;
+    const int rows = cout_write > 0 ? cout_write : a.cout;
+    const int total = rows * a.k_real;
     k_wgrad_reduce<<<(total + 255) / 256, 256, 0, s>>>(a.partial, (int)splits, a.k_pad, nt,
-                                                       a.cout, a.k_real, dw, accumulate);
+                                                       rows, a.k_real, dw, accumulate);
     return cudaGetLastError();
 }
 

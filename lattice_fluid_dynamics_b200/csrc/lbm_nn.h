@@ -14,8 +14,9 @@ struct ConvWgradArgs;
 // K (27 taps x cin) rounded up to a multiple of 128
 int k_pad_of(int cin);
 cudaError_t conv_forward(const ConvFwdArgs &a, int nt, cudaStream_t s);
+// dw rows written: cout_write (> 0) or a.cout
 cudaError_t conv_wgrad(const ConvWgradArgs &a, int nt, unsigned splits, float *dw, int accumulate,
-                       cudaStream_t s);
+                       cudaStream_t s, int cout_write = 0);
 cudaError_t weight_transpose(const __nv_bfloat16 *w, int cout, int cin, __nv_bfloat16 *wt,
                              int wt_rows, cudaStream_t s);
 // reads and clears the device error word of the GEMM kernels (synchronous)
