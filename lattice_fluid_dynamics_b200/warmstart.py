@@ -1,0 +1,314 @@
+"""Learned warm start: train the warm-start network on solver snapshots and
+measure what it gains.
+
+Pipeline (all on the GPU, through this library's C ABI):
+
+1. Shapes: random unions (one or two disjoint closed meshes) of ellipsoids,
+   boxes and slanted boxes drawn from a seed, placed around world x = -2 the
+   way the reference driver places a model (simulation/src/main.c:341-349),
+   with U ~ U[0.04, 0.08] and Re ~ U[20, 100] on the body length.
+2. Snapshots: each training shape is solved from uniform flow at half the
+   evaluation resolution (regularized collision, periodic y/z, tau from Re
+   with the reference driver's 0.52 clamp), all shapes of a chunk advanced
+   together by LBM_BatchRun; the developed field is reduced to the network's
+   resolution (LBM_WarmNetGridTargets) beside its features
+   (LBM_WarmNetGridFeatures).
+3. Training: Adam on mean squared error over the snapshots, with the
+   network's own forward and backward kernels (LBM_WarmNetTrainStepDevice).
+4. Evaluation on held-out shapes at the full resolution: a cold FP32 run from
+   uniform flow until Cd is stationary gives the converged Cd; then the
+   steps and wall time for Cd to enter and stay within 0.5 % of it, for
+   (a) plain FP32 from uniform flow and (b) FP16 storage initialised by the
+   network (LBM_InitializeFromWarmNet), with fallback to uniform flow when
+   the warm-started run trips the stability guard or produces a non-finite
+   drag.
+
+    python -m lattice_fluid_dynamics_b200.warmstart --train 2000 --eval 100
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import sys
+import time
+
+import numpy as np
+
+from . import capi, geometry
+
+
+# ---------------------------------------------------------------------------
+# shapes
+
+def _primitive(rng, kind, center, size):
+    if kind == "ellipsoid":
+        v, f = geometry.ellipsoid_cells(center, size, 20, 20)
+    elif kind == "box":
+        v, f = geometry.slanted_box_cells(center, size, 0.0)
+    else:
+        v, f = geometry.slanted_box_cells(center, size, float(rng.uniform(15, 35)))
+    return np.asarray(v, np.float64), f
+
+
+def random_union(seed: int, index: int) -> dict:
+    """One shape in world coordinates: a main primitive and, half of the
+    time, a second disjoint one downstream or beside it."""
+    rng = np.random.default_rng([seed, index])
+    kinds = ("ellipsoid", "box", "slanted_box")
+    k1 = kinds[int(rng.integers(0, 3))]
+    s1 = np.array([rng.uniform(0.5, 1.3), rng.uniform(0.3, 0.8), rng.uniform(0.3, 0.8)])
+    c1 = np.array([-2.0, rng.uniform(-0.15, 0.15), rng.uniform(-0.15, 0.15)])
+    parts = [_primitive(rng, k1, c1, s1)]
+    if rng.random() < 0.5:
+        k2 = kinds[int(rng.integers(0, 3))]
+        s2 = np.array([rng.uniform(0.25, 0.6), rng.uniform(0.2, 0.5), rng.uniform(0.2, 0.5)])
+        if rng.random() < 0.5:  # downstream, with a gap
+            c2 = c1 + [(s1[0] + s2[0]) / 2 + rng.uniform(0.15, 0.5), rng.uniform(-0.2, 0.2), 0]
+        else:                   # beside, with a gap
+            side = 1 if rng.random() < 0.5 else -1
+            c2 = c1 + [rng.uniform(-0.3, 0.3), side * ((s1[1] + s2[1]) / 2 + rng.uniform(0.1, 0.3)),
+                       0]
+        parts.append(_primitive(rng, k2, c2, s2))
+    tris, verts = [], []
+    for v, f in parts:
+        t = np.zeros((len(f), 12), np.float32)
+        fa = np.asarray(f)
+        t[:, 0:3], t[:, 4:7], t[:, 8:11] = v[fa[:, 0]], v[fa[:, 1]], v[fa[:, 2]]
+        tris.append(t)
+        verts.append(v)
+    v = np.concatenate(verts)
+    lo, hi = v.min(0), v.max(0)
+    return dict(index=index, triangles=np.concatenate(tris),
+                bbox=tuple(float(x) for x in (*lo, *hi)), length_world=float(hi[0] - lo[0]),
+                U=float(rng.uniform(0.04, 0.08)), Re=float(rng.uniform(20, 100)))
+
+
+def make_grid(shape: dict, dims, storage: str = "fp32", warm=None) -> capi.Grid:
+    nx, ny, nz = dims
+    L_cells = shape["length_world"] * nx / 8.0
+    _, nu, _, _ = capi.reynolds_to_tau(shape["U"], L_cells, shape["Re"])
+    g = capi.Grid(nx, ny, nz, nu, storage=storage)
+    g.set(useRegularized=1, periodicYZ=1)
+    g.set_solid_mesh(shape["triangles"], shape["bbox"])
+    return g
+
+
+# ---------------------------------------------------------------------------
+# snapshots
+
+def make_dataset(count: int, seed: int, dims=(128, 64, 64), steps: int = 6000,
+                 chunk: int = 64, factor: int = 2):
+    """Features [count, vox, 3] and targets [count, vox, 4] as CUDA tensors."""
+    import torch
+    nx, ny, nz = dims
+    vox = (nx // factor) * (ny // factor) * (nz // factor)
+    feats = torch.zeros((count, vox, 3), dtype=torch.float32, device="cuda")
+    tgts = torch.zeros((count, vox, 4), dtype=torch.float32, device="cuda")
+    L = capi.load()
+    resets = 0
+    for c0 in range(0, count, chunk):
+        shapes = [random_union(seed, i) for i in range(c0, min(count, c0 + chunk))]
+        grids = [make_grid(s, dims) for s in shapes]
+        for s, g in zip(shapes, grids):
+            g.initialize_flow(s["U"])
+        b = capi.Batch(grids)
+        b.run(steps, np.array([[s["U"], 0, 0] for s in shapes], np.float32))
+        for k, (s, g) in enumerate(zip(shapes, grids)):
+            i = c0 + k
+            rc1 = L.LBM_WarmNetGridFeatures(g.handle, factor, s["U"], s["Re"],
+                                            feats[i].data_ptr())
+            rc2 = L.LBM_WarmNetGridTargets(g.handle, factor, s["U"], tgts[i].data_ptr())
+            assert rc1 == 0 and rc2 == 0
+            resets += g.guard_resets()
+        b.close()
+        for g in grids:
+            g.close()
+    return feats, tgts, resets
+
+
+# ---------------------------------------------------------------------------
+# training
+
+def train(net: capi.WarmNet, feats, tgts, epochs: int, batch: int, lr: float, seed: int = 0,
+          val=None):
+    import torch
+    n = feats.shape[0]
+    rng = np.random.default_rng(seed)
+    steps = epochs * (n // batch)
+    history, t0, s = [], time.perf_counter(), 0
+    fb = torch.empty((batch,) + tuple(feats.shape[1:]), dtype=torch.float32, device="cuda")
+    tb = torch.empty((batch,) + tuple(tgts.shape[1:]), dtype=torch.float32, device="cuda")
+    for ep in range(epochs):
+        perm = torch.from_numpy(rng.permutation(n)).cuda()
+        losses = []
+        for j in range(n // batch):
+            idx = perm[j * batch:(j + 1) * batch]
+            torch.index_select(feats, 0, idx, out=fb)
+            torch.index_select(tgts, 0, idx, out=tb)
+            torch.cuda.synchronize()
+            lr_s = lr * 0.5 * (1 + math.cos(math.pi * s / steps))  # cosine decay
+            losses.append(net.train_step_device(fb.data_ptr(), tb.data_ptr(), batch, lr_s))
+            s += 1
+        rec = {"epoch": ep, "train_loss": float(np.mean(losses))}
+        if val is not None:
+            rec["val_loss"] = evaluate_loss(net, *val)
+        history.append(rec)
+    return history, time.perf_counter() - t0
+
+
+def evaluate_loss(net: capi.WarmNet, feats, tgts) -> float:
+    out = []
+    for i in range(feats.shape[0]):
+        loss, _ = net.loss_grad(feats[i].cpu().numpy(), tgts[i].cpu().numpy(), want_grad=False)
+        out.append(loss)
+    return float(np.mean(out))
+
+
+# ---------------------------------------------------------------------------
+# evaluation
+
+def _run_until_stationary(g: capi.Grid, U: float, area: float, sample: int, max_steps: int,
+                          tol: float = 1e-4, window: int = 10):
+    """Cd every `sample` steps until its spread over `window` samples falls
+    below tol (relative) or max_steps; returns (steps, cd list, host times)."""
+    import torch
+    cds, times = [], []
+    t0 = time.perf_counter()
+    done = 0
+    while done < max_steps:
+        g.step(U, n=sample)
+        done += sample
+        cds.append(float(g.drag_coefficient(U, area)))
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+        if not math.isfinite(cds[-1]):
+            break
+        if len(cds) >= window:
+            w = np.array(cds[-window:])
+            if (w.max() - w.min()) <= tol * abs(w.mean()):
+                break
+    return done, cds, times
+
+
+def _entry(cds, ref, band=0.005):
+    """Index of the first sample after which Cd stays within band of ref."""
+    ok = np.abs(np.array(cds) - ref) <= band * abs(ref)
+    for i in range(len(cds)):
+        if ok[i:].all():
+            return i
+    return None
+
+
+def evaluate(net: capi.WarmNet, shapes, dims=(256, 128, 128), sample: int = 100,
+             max_steps: int = 40000, warm_storage: str = "fp16"):
+    import torch
+    rows = []
+    for s in shapes:
+        U = s["U"]
+        # cold FP32 reference (the plain path)
+        g = make_grid(s, dims, "fp32")
+        area = g.projected_area(0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g.initialize_flow(U)
+        init_cold = time.perf_counter() - t0
+        n_c, cd_c, t_c = _run_until_stationary(g, U, area, sample, max_steps)
+        g.close()
+        ref = float(np.mean(cd_c[-5:]))
+        ic = _entry(cd_c, ref)
+        # warm start with reduced-precision storage
+        g = make_grid(s, dims, warm_storage)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc = capi.load().LBM_InitializeFromWarmNet(g.handle, net.handle, U, s["Re"])
+        torch.cuda.synchronize()
+        init_warm = time.perf_counter() - t0
+        fallback = False
+        if rc != 0:
+            g.initialize_flow(U)
+            fallback = True
+        n_w, cd_w, t_w = _run_until_stationary(g, U, area, sample, max_steps)
+        if not fallback and (g.guard_resets() > 0 or not all(map(math.isfinite, cd_w))):
+            # instability: plain start from uniform flow
+            g.initialize_flow(U)
+            fallback = True
+            n_w, cd_w, t_w = _run_until_stationary(g, U, area, sample, max_steps)
+        g.close()
+        iw = _entry(cd_w, ref)
+        row = {
+            "index": s["index"], "U": U, "Re": s["Re"], "cd_ref": ref,
+            "cold_steps": None if ic is None else (ic + 1) * sample,
+            "cold_wall_s": None if ic is None else init_cold + t_c[ic],
+            "cold_total_steps": n_c,
+            "warm_steps": None if iw is None else (iw + 1) * sample,
+            "warm_wall_s": None if iw is None else init_warm + t_w[iw],
+            "warm_init_s": init_warm, "warm_total_steps": n_w, "fallback": fallback,
+            "warm_cd_first": cd_w[0] if cd_w else None, "cold_cd_first": cd_c[0],
+        }
+        rows.append(row)
+    return rows
+
+
+def summarize(rows):
+    ok = [r for r in rows if r["cold_steps"] and r["warm_steps"]]
+    if not ok:
+        return {"evaluated": len(rows), "both_converged": 0}
+    cs = np.array([r["cold_steps"] for r in ok], float)
+    ws = np.array([r["warm_steps"] for r in ok], float)
+    ct = np.array([r["cold_wall_s"] for r in ok], float)
+    wt = np.array([r["warm_wall_s"] for r in ok], float)
+    return {
+        "evaluated": len(rows), "both_converged": len(ok),
+        "fallbacks": int(sum(r["fallback"] for r in rows)),
+        "cold_steps_median": float(np.median(cs)), "warm_steps_median": float(np.median(ws)),
+        "cold_wall_s_median": float(np.median(ct)), "warm_wall_s_median": float(np.median(wt)),
+        "wall_ratio_median": float(np.median(wt / ct)),
+        "wall_ratio_total": float(wt.sum() / ct.sum()),
+        "steps_ratio_total": float(ws.sum() / cs.sum()),
+    }
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--train", type=int, default=2000)
+    ap.add_argument("--val", type=int, default=64)
+    ap.add_argument("--eval", type=int, default=100)
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--snapshot-steps", type=int, default=6000)
+    ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--grid", default="256x128x128")
+    ap.add_argument("--max-steps", type=int, default=40000)
+    ap.add_argument("--sample", type=int, default=100)
+    ap.add_argument("--out", default="")
+    a = ap.parse_args(argv)
+    full = tuple(int(v) for v in a.grid.split("x"))
+    half = tuple(v // 2 for v in full)
+    res = {"grid": list(full), "snapshot_grid": list(half), "train": a.train, "seed": a.seed}
+    t0 = time.perf_counter()
+    feats, tgts, resets = make_dataset(a.train + a.val, a.seed, half, a.snapshot_steps)
+    res["dataset_s"] = time.perf_counter() - t0
+    res["dataset_guard_resets"] = resets
+    net = capi.WarmNet(full[0] // 4, full[1] // 4, full[2] // 4, max_batch=a.batch, seed=a.seed)
+    hist, tsec = train(net, feats[:a.train], tgts[:a.train], a.epochs, a.batch, a.lr,
+                       val=(feats[a.train:], tgts[a.train:]))
+    res["train_s"] = tsec
+    res["history"] = hist
+    # held-out shapes: indices beyond the training and validation ones
+    shapes = [random_union(a.seed, 100000 + i) for i in range(a.eval)]
+    rows = evaluate(net, shapes, full, a.sample, a.max_steps)
+    res["rows"] = rows
+    res["summary"] = summarize(rows)
+    print(json.dumps({k: v for k, v in res.items() if k not in ("rows", "history")} |
+                     {"final": hist[-1] if hist else None}))
+    if a.out:
+        with open(a.out, "w") as fh:
+            json.dump(res, fh, indent=1)
+        np.save(a.out.replace(".json", "_params.npy"), net.params())
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

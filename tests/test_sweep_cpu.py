@@ -44,3 +44,17 @@ def test_sweep_instances_deterministic_and_in_range():
 def test_sweep_meshes_closed():
     for i in geometry.sweep_instances(1, 12):
         assert _closed(i["triangles"]), i["kind"]
+
+
+def test_warmstart_shapes_closed_disjoint_deterministic():
+    from lattice_fluid_dynamics_b200 import warmstart as ws
+    for i in range(24):
+        a = ws.random_union(2, i)
+        b = ws.random_union(2, i)
+        assert np.array_equal(a["triangles"], b["triangles"]) and a["U"] == b["U"]
+        assert _closed(a["triangles"])
+        lo, hi = np.array(a["bbox"][:3]), np.array(a["bbox"][3:])
+        assert np.all(lo > [-4, -2, -2]) and np.all(hi < [0, 2, 2])
+        assert 0.04 <= a["U"] <= 0.08 and 20 <= a["Re"] <= 100
+    assert not np.array_equal(ws.random_union(2, 0)["triangles"],
+                              ws.random_union(2, 100000)["triangles"])
