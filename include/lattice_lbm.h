@@ -396,8 +396,11 @@ int LBM_WarmNetGridTargets(LBMGrid *grid, int factor, float U, float *targetDev)
 /* Warm start: run the network on the grid's mask (grid = factor x network
  * resolution on every axis), interpolate its prediction trilinearly to the
  * grid, and initialise f = f_new = feq(rho, u) (solid cells rho = 1, u = 0)
- * -- LBM_InitializeFlow with a predicted field instead of a uniform one. */
-int LBM_InitializeFromWarmNet(LBMGrid *grid, LBMWarmNet *net, float U, float Re);
+ * -- LBM_InitializeFlow with a predicted field instead of a uniform one.
+ * flags: LBM_WARM_UNIFORM_DENSITY keeps rho = 1 and takes only the
+ * predicted velocity. */
+#define LBM_WARM_UNIFORM_DENSITY 1
+int LBM_InitializeFromWarmNet(LBMGrid *grid, LBMWarmNet *net, float U, float Re, int flags);
 
 /* ---------------------------------------------------------------------
  * Host side of the driver: OBJ ingestion, model placement, Re -> tau,

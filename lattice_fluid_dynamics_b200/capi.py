@@ -173,7 +173,7 @@ SIGNATURES = {
     "LBM_WarmNetGetStream": (_vp, [_vp]),
     "LBM_WarmNetGridFeatures": (C.c_int, [_G, C.c_int, _f, _f, _vp]),
     "LBM_WarmNetGridTargets": (C.c_int, [_G, C.c_int, _f, _vp]),
-    "LBM_InitializeFromWarmNet": (C.c_int, [_G, _vp, _f, _f]),
+    "LBM_InitializeFromWarmNet": (C.c_int, [_G, _vp, _f, _f, C.c_int]),
     "LBM_CdMonitorInit": (None, [_vp]),
     "LBM_CdMonitorAdd": (C.c_int, [_vp, _f, _f]),
     "LBM_TunnelCoefficients": (None, [_f, _f, _f, _f, _f, _f, _vp]),

@@ -276,10 +276,12 @@ __global__ void k_grid_targets(const float4 *__restrict__ vel, const int32_t *__
 
 // full-resolution (rho, u) from the prediction at 1/f resolution: trilinear
 // interpolation at cell centres ((x + 0.5) / f - 0.5, clamped), decoded as
-// rho = 1 + U^2 p0, u = U (p1, p2, p3); solid cells rho = 1, u = 0
+// rho = 1 + U^2 p0 (or 1 when use_density is 0), u = U (p1, p2, p3); solid
+// cells rho = 1, u = 0
 __global__ void k_decode_upsample(const float *__restrict__ pred, int nx, int ny, int nz, int f,
                                   float U, const int32_t *__restrict__ solid, int NX, int NY,
-                                  int NZ, float *__restrict__ rho, float *__restrict__ u) {
+                                  int NZ, float *__restrict__ rho, float *__restrict__ u,
+                                  int use_density) {
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= (long long)NX * NY * NZ) return;
     const int X = (int)(c % NX), Y = (int)((c / NX) % NY), Z = (int)(c / ((long long)NX * NY));
@@ -307,7 +309,7 @@ __global__ void k_decode_upsample(const float *__restrict__ pred, int nx, int ny
         const float c11 = P(z1, y1, x0) * (1 - fx) + P(z1, y1, x1) * fx;
         o[k] = (c00 * (1 - fy) + c01 * fy) * (1 - fz) + (c10 * (1 - fy) + c11 * fy) * fz;
     }
-    rho[c] = 1.f + U * U * o[0];
+    rho[c] = use_density ? 1.f + U * U * o[0] : 1.f;
     u[3 * c] = U * o[1];
     u[3 * c + 1] = U * o[2];
     u[3 * c + 2] = U * o[3];
@@ -865,7 +867,7 @@ int LBM_WarmNetGridTargets(LBMGrid *grid, int factor, float U, float *targetDev)
     return LBM_OK;
 }
 
-int LBM_InitializeFromWarmNet(LBMGrid *grid, LBMWarmNet *n, float U, float Re) {
+int LBM_InitializeFromWarmNet(LBMGrid *grid, LBMWarmNet *n, float U, float Re, int flags) {
     if (!grid || !grid->impl || !n || !(U > 0.f) || !(Re > 0.f)) return LBM_ERR_INVALID_ARGUMENT;
     GridImpl &I = *static_cast<GridImpl *>(grid->impl);
     if (I.nx % n->nx || I.nx / n->nx != I.ny / n->ny || I.nx / n->nx != I.nz / n->nz ||
@@ -880,7 +882,8 @@ int LBM_InitializeFromWarmNet(LBMGrid *grid, LBMWarmNet *n, float U, float Re) {
     if (cudaMallocAsync(&d, sizeof(float) * 4 * (size_t)I.n, I.stream) != cudaSuccess)
         return LBM_ERR_OUT_OF_MEMORY;
     k_decode_upsample<<<nblk(I.n), 256, 0, I.stream>>>(n->pred32, n->nx, n->ny, n->nz, f, U,
-                                                       I.solid, I.nx, I.ny, I.nz, d, d + I.n);
+                                                       I.solid, I.nx, I.ny, I.nz, d, d + I.n,
+                                                       (flags & LBM_WARM_UNIFORM_DENSITY) ? 0 : 1);
     rc = cudaGetLastError() == cudaSuccess && grid_init_from_device(grid, d, d + I.n) ? LBM_OK
                                                                                        : LBM_ERR_CUDA;
     cudaFreeAsync(d, I.stream);

@@ -103,14 +103,16 @@ def make_grid(shape: dict, dims, storage: str = "fp32") -> capi.Grid:
 
 def make_dataset(count: int, seed: int, dims=(128, 64, 64), steps: int = 6000,
                  chunk: int = 64, factor: int = 2):
-    """Features [count, vox, 3] and targets [count, vox, 4] as CUDA tensors."""
+    """Features [count, vox, 3] and targets [count, vox, 4] as CUDA tensors,
+    and each instance's stability-guard reset count (instances with resets
+    are left out of training)."""
     import torch
     nx, ny, nz = dims
     vox = (nx // factor) * (ny // factor) * (nz // factor)
     feats = torch.zeros((count, vox, 3), dtype=torch.float32, device="cuda")
     tgts = torch.zeros((count, vox, 4), dtype=torch.float32, device="cuda")
     L = capi.load()
-    resets = 0
+    resets = np.zeros(count, np.int64)
     for c0 in range(0, count, chunk):
         shapes = [random_union(seed, i) for i in range(c0, min(count, c0 + chunk))]
         grids = [make_grid(s, dims) for s in shapes]
@@ -124,7 +126,7 @@ def make_dataset(count: int, seed: int, dims=(128, 64, 64), steps: int = 6000,
                                             feats[i].data_ptr())
             rc2 = L.LBM_WarmNetGridTargets(g.handle, factor, s["U"], tgts[i].data_ptr())
             assert rc1 == 0 and rc2 == 0
-            resets += g.guard_resets()
+            resets[i] = g.guard_resets()
         b.close()
         for g in grids:
             g.close()
@@ -208,17 +210,30 @@ def entry_index(avg, ref, band=0.005):
     return i if i < len(avg) else None
 
 
+VARIANTS = {
+    "cold_fp32": ("fp32", "cold"),   # the plain path
+    "warm_fp16": ("fp16", "warm"),   # learned warm start + FP16 storage
+    "warm_fp32": ("fp32", "warm"),
+    "warmu_fp16": ("fp16", "warm_velocity"),
+    "cold_fp16": ("fp16", "cold"),
+}
+
+
 def evaluate(net: capi.WarmNet, shapes, dims=(256, 128, 128), sample: int = 50,
              cold_steps: int = 30000, avg_steps: int = 2000, ref_steps: int = 5000,
-             hold_steps: int = 5000, warm_storage: str = "fp16"):
+             hold_steps: int = 5000, variants=("warm_fp16",)):
     """Per shape: the converged Cd (mean of the raw Cd over the last
-    ref_steps of a cold FP32 run of cold_steps), and for the cold FP32 run and
-    the warm-started run the steps and wall time until the Cd averaged over
-    the trailing avg_steps enters and stays within 0.5 % of it.  The warm
-    run stops once it has stayed in the band for hold_steps."""
+    ref_steps of a cold FP32 run of cold_steps) and, for the cold FP32 run
+    and every variant, the steps and wall time until the Cd averaged over the
+    trailing avg_steps enters and stays within 0.5 % of it (a variant's run
+    stops once it has stayed in the band for hold_steps).  Warm variants fall
+    back to uniform flow when the warm-started run trips the stability guard
+    or its drag is not finite."""
     import torch
     rows = []
     w = max(1, avg_steps // sample)
+    hold = max(1, hold_steps // sample)
+    L = capi.load()
     for s in shapes:
         U = s["U"]
         g = make_grid(s, dims, "fp32")
@@ -232,7 +247,12 @@ def evaluate(net: capi.WarmNet, shapes, dims=(256, 128, 128), sample: int = 50,
         g.close()
         ref = float(np.mean(cd_c[-max(1, ref_steps // sample):]))
         ic = entry_index(smoothed(cd_c, w), ref)
-        hold = max(1, hold_steps // sample)
+        row = {"index": s["index"], "U": U, "Re": s["Re"], "cd_ref": ref,
+               "cold_fp32": {"steps": None if ic is None else (ic + 1) * sample,
+                             "wall_s": None if ic is None else init_cold + t_c[ic],
+                             "ms_per_step": 1e3 * t_c[-1] / (len(t_c) * sample),
+                             "guard_resets": cold_resets,
+                             "series": [round(v, 5) for v in smoothed(cd_c, w)[::10]]}}
 
         def stop(cds):
             if len(cds) < w:
@@ -240,53 +260,60 @@ def evaluate(net: capi.WarmNet, shapes, dims=(256, 128, 128), sample: int = 50,
             e = entry_index(smoothed(cds, w), ref)
             return e is not None and len(cds) - e >= hold
 
-        g = make_grid(s, dims, warm_storage)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        rc = capi.load().LBM_InitializeFromWarmNet(g.handle, net.handle, U, s["Re"])
-        torch.cuda.synchronize()
-        init_warm = time.perf_counter() - t0
-        fallback = rc != 0
-        if fallback:
-            g.initialize_flow(U)
-        cd_w, t_w = _run(g, U, area, sample, cold_steps, stop)
-        if not fallback and (g.guard_resets() > 0 or not all(map(math.isfinite, cd_w))):
-            g.initialize_flow(U)  # unstable warm start: plain start from uniform flow
-            fallback = True
-            cd_w, t_w = _run(g, U, area, sample, cold_steps, stop)
-        g.close()
-        iw = entry_index(smoothed(cd_w, w), ref)
-        rows.append({
-            "index": s["index"], "U": U, "Re": s["Re"], "cd_ref": ref,
-            "cold_steps": None if ic is None else (ic + 1) * sample,
-            "cold_wall_s": None if ic is None else init_cold + t_c[ic],
-            "cold_ms_per_step": 1e3 * t_c[-1] / (len(t_c) * sample),
-            "warm_steps": None if iw is None else (iw + 1) * sample,
-            "warm_wall_s": None if iw is None else init_warm + t_w[iw],
-            "warm_ms_per_step": 1e3 * t_w[-1] / (len(t_w) * sample),
-            "warm_init_s": init_warm, "fallback": fallback, "cold_guard_resets": cold_resets,
-            "cd_first_cold": cd_c[0], "cd_first_warm": cd_w[0] if cd_w else None,
-        })
+        for name in variants:
+            storage, init = VARIANTS[name]
+            g = make_grid(s, dims, storage)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fallback = False
+            if init == "cold":
+                g.initialize_flow(U)
+            else:
+                flags = 1 if init == "warm_velocity" else 0
+                if L.LBM_InitializeFromWarmNet(g.handle, net.handle, U, s["Re"], flags) != 0:
+                    g.initialize_flow(U)
+                    fallback = True
+            torch.cuda.synchronize()
+            t_init = time.perf_counter() - t0
+            cd_v, t_v = _run(g, U, area, sample, cold_steps, stop)
+            if init != "cold" and not fallback and (
+                    g.guard_resets() > 0 or not all(map(math.isfinite, cd_v))):
+                g.initialize_flow(U)  # unstable warm start: plain start from uniform flow
+                fallback = True
+                cd_v, t_v = _run(g, U, area, sample, cold_steps, stop)
+            g.close()
+            iv = entry_index(smoothed(cd_v, w), ref)
+            row[name] = {"steps": None if iv is None else (iv + 1) * sample,
+                         "wall_s": None if iv is None else t_init + t_v[iv],
+                         "init_s": t_init, "fallback": fallback,
+                         "ms_per_step": 1e3 * t_v[-1] / (len(t_v) * sample),
+                         "cd_end": float(np.mean(cd_v[-w:])),
+                         "series": [round(v, 5) for v in smoothed(cd_v, w)[::10]]}
+        rows.append(row)
     return rows
 
 
-def summarize(rows):
-    ok = [r for r in rows if r["cold_steps"] and r["warm_steps"]]
+def summarize(rows, variant="warm_fp16"):
+    """Medians and totals of steps / wall time to the 0.5 % band, `variant`
+    against the plain cold FP32 path, over shapes where both entered it."""
+    ok = [r for r in rows if r["cold_fp32"]["steps"] and r.get(variant, {}).get("steps")]
+    out = {"variant": variant, "evaluated": len(rows), "both_converged": len(ok),
+           "fallbacks": int(sum(r.get(variant, {}).get("fallback", False) for r in rows))}
     if not ok:
-        return {"evaluated": len(rows), "both_converged": 0}
-    cs = np.array([r["cold_steps"] for r in ok], float)
-    ws = np.array([r["warm_steps"] for r in ok], float)
-    ct = np.array([r["cold_wall_s"] for r in ok], float)
-    wt = np.array([r["warm_wall_s"] for r in ok], float)
-    return {
-        "evaluated": len(rows), "both_converged": len(ok),
-        "fallbacks": int(sum(r["fallback"] for r in rows)),
-        "cold_steps_median": float(np.median(cs)), "warm_steps_median": float(np.median(ws)),
-        "cold_wall_s_median": float(np.median(ct)), "warm_wall_s_median": float(np.median(wt)),
-        "wall_ratio_median": float(np.median(wt / ct)),
-        "wall_ratio_total": float(wt.sum() / ct.sum()),
-        "steps_ratio_total": float(ws.sum() / cs.sum()),
-    }
+        return out
+    cs = np.array([r["cold_fp32"]["steps"] for r in ok], float)
+    vs = np.array([r[variant]["steps"] for r in ok], float)
+    ct = np.array([r["cold_fp32"]["wall_s"] for r in ok], float)
+    vt = np.array([r[variant]["wall_s"] for r in ok], float)
+    out.update({
+        "cold_steps_median": float(np.median(cs)), "steps_median": float(np.median(vs)),
+        "cold_wall_s_median": float(np.median(ct)), "wall_s_median": float(np.median(vt)),
+        "wall_ratio_median": float(np.median(vt / ct)),
+        "wall_ratio_total": float(vt.sum() / ct.sum()),
+        "steps_ratio_total": float(vs.sum() / cs.sum()),
+        "faster_fraction": float(np.mean(vt < ct)),
+    })
+    return out
 
 
 def main(argv=None) -> int:
@@ -302,25 +329,26 @@ def main(argv=None) -> int:
     ap.add_argument("--grid", default="256x128x128")
     ap.add_argument("--cold-steps", type=int, default=30000)
     ap.add_argument("--sample", type=int, default=50)
+    ap.add_argument("--variants", default="warm_fp16",
+                    help="comma list of " + ",".join(VARIANTS))
+    ap.add_argument("--params", default="", help="trained parameters (.npy): skip training")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     full = tuple(int(v) for v in a.grid.split("x"))
     half = tuple(v // 2 for v in full)
     res = {"grid": list(full), "snapshot_grid": list(half), "train": a.train, "seed": a.seed}
-    t0 = time.perf_counter()
-    feats, tgts, resets = make_dataset(a.train + a.val, a.seed, half, a.snapshot_steps)
-    res["dataset_s"] = time.perf_counter() - t0
-    res["dataset_guard_resets"] = resets
     net = capi.WarmNet(full[0] // 4, full[1] // 4, full[2] // 4, max_batch=a.batch, seed=a.seed)
-    hist, tsec = train(net, feats[:a.train], tgts[:a.train], a.epochs, a.batch, a.lr,
-                       val=(feats[a.train:], tgts[a.train:]))
-    res["train_s"] = tsec
-    res["history"] = hist
+    hist = []
+    if a.params:
+        net.set_params(np.load(a.params))
+    else:
+        hist = _train_from_snapshots(net, a, half, res)
     # held-out shapes: indices beyond the training and validation ones
     shapes = [random_union(a.seed, 100000 + i) for i in range(a.eval)]
-    rows = evaluate(net, shapes, full, a.sample, a.cold_steps)
+    variants = tuple(a.variants.split(","))
+    rows = evaluate(net, shapes, full, a.sample, a.cold_steps, variants=variants)
     res["rows"] = rows
-    res["summary"] = summarize(rows)
+    res["summary"] = {v: summarize(rows, v) for v in variants}
     print(json.dumps({k: v for k, v in res.items() if k not in ("rows", "history")} |
                      {"final": hist[-1] if hist else None}))
     if a.out:
@@ -328,6 +356,30 @@ def main(argv=None) -> int:
             json.dump(res, fh, indent=1)
         np.save(a.out.replace(".json", "_params.npy"), net.params())
     return 0
+
+
+def _train_from_snapshots(net, a, half, res):
+    t0 = time.perf_counter()
+    feats, tgts, resets = make_dataset(a.train + a.val, a.seed, half, a.snapshot_steps)
+    res["dataset_s"] = time.perf_counter() - t0
+    res["dataset_unstable"] = int((resets > 0).sum())
+    res["dataset_unstable_shapes"] = [
+        {k: v for k, v in random_union(a.seed, int(i)).items() if k in ("index", "U", "Re",
+                                                                      "length_world")}
+        for i in np.nonzero(resets > 0)[0][:20]]
+    keep = np.nonzero(resets == 0)[0]
+    import torch
+    kt = torch.from_numpy(keep).cuda()
+    feats, tgts = feats.index_select(0, kt), tgts.index_select(0, kt)
+    ntr = int(round(len(keep) * a.train / (a.train + a.val)))
+    t = tgts.reshape(-1, 4)
+    res["target_stats"] = {"mean": t.mean(0).tolist(), "std": t.std(0).tolist(),
+                           "min": t.min(0).values.tolist(), "max": t.max(0).values.tolist()}
+    hist, tsec = train(net, feats[:ntr], tgts[:ntr], a.epochs, a.batch, a.lr,
+                       val=(feats[ntr:], tgts[ntr:]))
+    res["train_s"] = tsec
+    res["history"] = hist
+    return hist
 
 
 if __name__ == "__main__":

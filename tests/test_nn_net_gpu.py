@@ -101,7 +101,7 @@ def test_warm_initialisation_decodes_prediction(solver):
     g = capi.Grid(64, 32, 32, 0.02)
     g.set_solid_sphere(-2.0, 0.0, 0.0, 0.5)
     U = 0.04
-    assert capi.load().LBM_InitializeFromWarmNet(g.handle, net.handle, U, 300.0) == 0
+    assert capi.load().LBM_InitializeFromWarmNet(g.handle, net.handle, U, 300.0, 0) == 0
     vel = g.velocity()
     solid = g.solid()
     fl = solid == 0
@@ -110,6 +110,10 @@ def test_warm_initialisation_decodes_prediction(solver):
     assert np.all(vel[~fl, :3] == 0) and np.all(vel[~fl, 3] == 1)
     g.step(U, n=20)
     assert np.isfinite(g.drag_force_decomposed()).all()
+    # velocity only: density stays 1
+    assert capi.load().LBM_InitializeFromWarmNet(g.handle, net.handle, U, 300.0, 1) == 0
+    vel = g.velocity()
+    assert np.allclose(vel[fl, 0], U, rtol=1e-6) and np.all(vel[:, 3] == 1)
 
 
 @pytest.mark.gpu
