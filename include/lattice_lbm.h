@@ -398,8 +398,12 @@ int LBM_WarmNetGridTargets(LBMGrid *grid, int factor, float U, float *targetDev)
  * grid, and initialise f = f_new = feq(rho, u) (solid cells rho = 1, u = 0)
  * -- LBM_InitializeFlow with a predicted field instead of a uniform one.
  * flags: LBM_WARM_UNIFORM_DENSITY keeps rho = 1 and takes only the
- * predicted velocity. */
+ * predicted velocity; LBM_WARM_FLUX_CORRECT then shifts u_x in every
+ * x-plane so that it carries the inlet mass flux U * NY * NZ and shifts rho
+ * so that the outlet plane's mean is 1 (continuity of the initial field,
+ * which otherwise launches a tunnel-length pressure wave). */
 #define LBM_WARM_UNIFORM_DENSITY 1
+#define LBM_WARM_FLUX_CORRECT 2
 int LBM_InitializeFromWarmNet(LBMGrid *grid, LBMWarmNet *net, float U, float Re, int flags);
 
 /* ---------------------------------------------------------------------

@@ -231,6 +231,52 @@ __global__ void k_pred_out(const __nv_bfloat16 *__restrict__ pred, long long m,
 
 inline unsigned nblk(long long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
+// Per x-plane sums of a full-resolution field: flux rho * u_x over all
+// cells, fluid-cell count, and the density sum over fluid cells.  One block
+// per plane, fixed summation order.
+__global__ void k_plane_sums(const float *__restrict__ rho, const float *__restrict__ u,
+                             const int32_t *__restrict__ solid, int NX, int NY, int NZ,
+                             double *__restrict__ out) {
+    const int x = blockIdx.x;
+    double flux = 0.0, cnt = 0.0, rs = 0.0;
+    for (long long q = threadIdx.x; q < (long long)NY * NZ; q += blockDim.x) {
+        const long long c = q * NX + x;
+        flux += (double)rho[c] * u[3 * c];
+        if (solid[c] == 0) {
+            cnt += 1.0;
+            rs += rho[c];
+        }
+    }
+    __shared__ double sh[3][256];
+    sh[0][threadIdx.x] = flux;
+    sh[1][threadIdx.x] = cnt;
+    sh[2][threadIdx.x] = rs;
+    __syncthreads();
+    for (int st = 128; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st)
+            for (int k = 0; k < 3; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x < 3) out[3 * x + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+// Continuity: shift u_x of the fluid cells of every x-plane so that the
+// plane carries the inlet mass flux U * NY * NZ, and shift the density so
+// that the outlet plane's fluid mean is the outlet's rho = 1.
+__global__ void k_flux_correct(float *__restrict__ rho, float *__restrict__ u,
+                               const int32_t *__restrict__ solid, int NX, int NY, int NZ, float U,
+                               const double *__restrict__ sums) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (long long)NX * NY * NZ || solid[c] != 0) return;
+    const int x = (int)(c % NX);
+    const double cnt = sums[3 * x + 1];
+    if (cnt <= 0.0) return;
+    const double target = (double)U * NY * NZ;
+    u[3 * c] += (float)((target - sums[3 * x]) / cnt);
+    const double cout_ = sums[3 * (NX - 1) + 1];
+    if (cout_ > 0.0) rho[c] += (float)(1.0 - sums[3 * (NX - 1) + 2] / cout_);
+}
+
 // features of a grid at 1/f resolution: solid fraction of each f^3 block
 // (cells with solid == 1), U and Re
 __global__ void k_grid_features(const int32_t *__restrict__ solid, int NX, int NY, int NZ, int f,
@@ -884,8 +930,19 @@ int LBM_InitializeFromWarmNet(LBMGrid *grid, LBMWarmNet *n, float U, float Re, i
     k_decode_upsample<<<nblk(I.n), 256, 0, I.stream>>>(n->pred32, n->nx, n->ny, n->nz, f, U,
                                                        I.solid, I.nx, I.ny, I.nz, d, d + I.n,
                                                        (flags & LBM_WARM_UNIFORM_DENSITY) ? 0 : 1);
-    rc = cudaGetLastError() == cudaSuccess && grid_init_from_device(grid, d, d + I.n) ? LBM_OK
-                                                                                       : LBM_ERR_CUDA;
+    bool good = cudaGetLastError() == cudaSuccess;
+    if (good && (flags & LBM_WARM_FLUX_CORRECT)) {
+        double *sums = nullptr;
+        good = cudaMallocAsync(&sums, sizeof(double) * 3 * I.nx, I.stream) == cudaSuccess;
+        if (good) {
+            k_plane_sums<<<I.nx, 256, 0, I.stream>>>(d, d + I.n, I.solid, I.nx, I.ny, I.nz, sums);
+            k_flux_correct<<<nblk(I.n), 256, 0, I.stream>>>(d, d + I.n, I.solid, I.nx, I.ny,
+                                                            I.nz, U, sums);
+            good = cudaGetLastError() == cudaSuccess;
+            cudaFreeAsync(sums, I.stream);
+        }
+    }
+    rc = good && grid_init_from_device(grid, d, d + I.n) ? LBM_OK : LBM_ERR_CUDA;
     cudaFreeAsync(d, I.stream);
     cudaStreamSynchronize(I.stream);
     return rc;

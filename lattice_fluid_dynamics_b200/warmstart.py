@@ -215,6 +215,8 @@ VARIANTS = {
     "warm_fp16": ("fp16", "warm"),   # learned warm start + FP16 storage
     "warm_fp32": ("fp32", "warm"),
     "warmu_fp16": ("fp16", "warm_velocity"),
+    "warmc_fp16": ("fp16", "warm_flux"),
+    "warmc_fp32": ("fp32", "warm_flux"),
     "cold_fp16": ("fp16", "cold"),
 }
 
@@ -269,7 +271,7 @@ def evaluate(net: capi.WarmNet, shapes, dims=(256, 128, 128), sample: int = 50,
             if init == "cold":
                 g.initialize_flow(U)
             else:
-                flags = 1 if init == "warm_velocity" else 0
+                flags = {"warm": 0, "warm_velocity": 1, "warm_flux": 2}[init]
                 if L.LBM_InitializeFromWarmNet(g.handle, net.handle, U, s["Re"], flags) != 0:
                     g.initialize_flow(U)
                     fallback = True
