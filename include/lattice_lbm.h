@@ -387,6 +387,11 @@ int LBM_WarmNetTrainStep(LBMWarmNet *net, const float *features, const float *ta
 int LBM_WarmNetTrainStepDevice(LBMWarmNet *net, const float *features, const float *target,
                                int batch, float lr, double *loss);
 void *LBM_WarmNetGetStream(LBMWarmNet *net);
+/* Predictions (LBM_WarmNetForward*, LBM_InitializeFromWarmNet) are
+ * shift + scale * network output per channel; training targets are given
+ * in the network's normalised units, (target - shift) / scale.  Default
+ * scale 1, shift 0. */
+int LBM_WarmNetSetOutputScaling(LBMWarmNet *net, const float *scale4, const float *shift4);
 /* Features / targets of a grid at 1/factor resolution into device arrays:
  * solid fraction of each factor^3 block with U and Re; block means of
  * ((rho - 1) / U^2, u / U) over fluid cells (solid cells count as rho = 1,

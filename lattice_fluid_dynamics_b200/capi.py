@@ -171,6 +171,7 @@ SIGNATURES = {
     "LBM_WarmNetTrainStep": (C.c_int, [_vp, _vp, _vp, C.c_int, _f, _vp]),
     "LBM_WarmNetTrainStepDevice": (C.c_int, [_vp, _vp, _vp, C.c_int, _f, _vp]),
     "LBM_WarmNetGetStream": (_vp, [_vp]),
+    "LBM_WarmNetSetOutputScaling": (C.c_int, [_vp, _vp, _vp]),
     "LBM_WarmNetGridFeatures": (C.c_int, [_G, C.c_int, _f, _f, _vp]),
     "LBM_WarmNetGridTargets": (C.c_int, [_G, C.c_int, _f, _vp]),
     "LBM_InitializeFromWarmNet": (C.c_int, [_G, _vp, _f, _f, C.c_int]),
@@ -682,6 +683,12 @@ class WarmNet:
         self._check(self._L.LBM_WarmNetTrainStep(self._n, _p(f), _p(t), b, lr, C.byref(loss)),
                     "train_step")
         return loss.value
+
+    def set_output_scaling(self, scale, shift):
+        sc = np.ascontiguousarray(scale, np.float32)
+        sh = np.ascontiguousarray(shift, np.float32)
+        self._check(self._L.LBM_WarmNetSetOutputScaling(self._n, _p(sc), _p(sh)),
+                    "LBM_WarmNetSetOutputScaling")
 
     def train_step_device(self, feat_ptr: int, target_ptr: int, batch: int, lr: float) -> float:
         loss = C.c_double()

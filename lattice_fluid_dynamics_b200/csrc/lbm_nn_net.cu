@@ -221,12 +221,17 @@ __global__ void k_pack(const float *__restrict__ w, const float *__restrict__ b,
     wb[i] = __float2bfloat16_rn((n < cout && k < kreal) ? w[(long long)n * kreal + k] : 0.f);
 }
 
-// pred [m][16] bf16 -> host layout [m][4] fp32
-__global__ void k_pred_out(const __nv_bfloat16 *__restrict__ pred, long long m,
+struct OutScale {
+    float scale[4], shift[4];
+};
+
+// pred [m][16] bf16 -> [m][4] fp32 in physical units: shift + scale * p
+__global__ void k_pred_out(const __nv_bfloat16 *__restrict__ pred, long long m, OutScale os,
                            float *__restrict__ out) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m * 4) return;
-    out[i] = __bfloat162float(pred[(i >> 2) * 16 + (i & 3)]);
+    const int k = (int)(i & 3);
+    out[i] = os.shift[k] + os.scale[k] * __bfloat162float(pred[(i >> 2) * 16 + k]);
 }
 
 inline unsigned nblk(long long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
@@ -392,6 +397,7 @@ struct LBMWarmNet {
     float *feat = nullptr, *target = nullptr, *pred32 = nullptr;
     double *loss = nullptr;
     int error = 0;
+    OutScale out_scale = {{1.f, 1.f, 1.f, 1.f}, {0.f, 0.f, 0.f, 0.f}};
 
     template <class T>
     T *alloc(long long n) {
@@ -805,7 +811,7 @@ int LBM_WarmNetForwardDevice(LBMWarmNet *n, const float *features, int batch, fl
     if (!valid_batch(n, batch) || !features || !pred) return LBM_ERR_INVALID_ARGUMENT;
     if (!forward(n, features, batch)) return LBM_ERR_CUDA;
     const long long m1 = n->m(0, batch);
-    k_pred_out<<<nblk(m1 * 4), 256, 0, n->stream>>>(n->pred, m1, pred);
+    k_pred_out<<<nblk(m1 * 4), 256, 0, n->stream>>>(n->pred, m1, n->out_scale, pred);
     return ok(n, cudaGetLastError()) ? finish(n) : LBM_ERR_CUDA;
 }
 
@@ -885,6 +891,15 @@ int LBM_WarmNetTrainStep(LBMWarmNet *n, const float *features, const float *targ
 }
 
 void *LBM_WarmNetGetStream(LBMWarmNet *n) { return n ? (void *)n->stream : nullptr; }
+
+int LBM_WarmNetSetOutputScaling(LBMWarmNet *n, const float *scale4, const float *shift4) {
+    if (!n || !scale4 || !shift4) return LBM_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < 4; k++) {
+        n->out_scale.scale[k] = scale4[k];
+        n->out_scale.shift[k] = shift4[k];
+    }
+    return LBM_OK;
+}
 
 int LBM_WarmNetGridFeatures(LBMGrid *grid, int factor, float U, float Re, float *featDev) {
     if (!grid || !grid->impl || factor <= 0 || !featDev) return LBM_ERR_INVALID_ARGUMENT;

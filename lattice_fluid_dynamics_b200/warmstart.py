@@ -334,6 +334,7 @@ def main(argv=None) -> int:
     ap.add_argument("--variants", default="warm_fp16",
                     help="comma list of " + ",".join(VARIANTS))
     ap.add_argument("--params", default="", help="trained parameters (.npy): skip training")
+    ap.add_argument("--scaling", default="", help="results .json holding the output scaling")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     full = tuple(int(v) for v in a.grid.split("x"))
@@ -343,6 +344,9 @@ def main(argv=None) -> int:
     hist = []
     if a.params:
         net.set_params(np.load(a.params))
+        if a.scaling:
+            sc = json.load(open(a.scaling))["output_scaling"]
+            net.set_output_scaling(sc["scale"], sc["shift"])
     else:
         hist = _train_from_snapshots(net, a, half, res)
     # held-out shapes: indices beyond the training and validation ones
@@ -377,6 +381,11 @@ def _train_from_snapshots(net, a, half, res):
     t = tgts.reshape(-1, 4)
     res["target_stats"] = {"mean": t.mean(0).tolist(), "std": t.std(0).tolist(),
                            "min": t.min(0).values.tolist(), "max": t.max(0).values.tolist()}
+    # every output channel in units of its spread over the training set
+    mean, std = t.mean(0), t.std(0).clamp_min(1e-6)
+    tgts = (tgts - mean) / std
+    net.set_output_scaling(std.cpu().numpy(), mean.cpu().numpy())
+    res["output_scaling"] = {"scale": std.tolist(), "shift": mean.tolist()}
     hist, tsec = train(net, feats[:ntr], tgts[:ntr], a.epochs, a.batch, a.lr,
                        val=(feats[ntr:], tgts[ntr:]))
     res["train_s"] = tsec

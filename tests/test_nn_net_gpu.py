@@ -110,6 +110,13 @@ def test_warm_initialisation_decodes_prediction(solver):
     assert np.all(vel[~fl, :3] == 0) and np.all(vel[~fl, 3] == 1)
     g.step(U, n=20)
     assert np.isfinite(g.drag_force_decomposed()).all()
+    # output scaling: physical = shift + scale * output
+    net.set_output_scaling([2.0, 0.5, 1.0, 1.0], [0.25, 0.5, 0.0, 0.0])
+    assert capi.load().LBM_InitializeFromWarmNet(g.handle, net.handle, U, 300.0, 0) == 0
+    vel = g.velocity()
+    assert np.allclose(vel[fl, 0], U, rtol=1e-6)  # 0.5 + 0.5 * 1
+    assert np.allclose(vel[fl, 3], np.float32(1 + 1.25 * U * U), rtol=1e-6)  # 0.25 + 2 * 0.5
+    net.set_output_scaling([1.0] * 4, [0.0] * 4)
     # velocity only: density stays 1
     assert capi.load().LBM_InitializeFromWarmNet(g.handle, net.handle, U, 300.0, 1) == 0
     vel = g.velocity()
@@ -140,3 +147,20 @@ def test_grid_features_and_targets(solver):
     q[sm] = 0
     ref = q.reshape(8, 2, 8, 2, 16, 2, 4).mean(axis=(1, 3, 5)).reshape(-1, 4)
     assert np.allclose(tgt.cpu().numpy(), ref, rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.gpu
+def test_warm_initialisation_flux_correction(solver):
+    """LBM_WARM_FLUX_CORRECT: every x-plane carries the inlet mass flux and
+    the outlet plane's fluid density averages 1."""
+    net = capi.WarmNet(16, 8, 8, max_batch=1, seed=4)  # untrained: an arbitrary field
+    g = capi.Grid(64, 32, 32, 0.02)
+    g.set_solid_sphere(-2.0, 0.0, 0.0, 0.6)
+    U = 0.05
+    assert capi.load().LBM_InitializeFromWarmNet(g.handle, net.handle, U, 300.0, 2) == 0
+    vel = g.velocity().reshape(32, 32, 64, 4).astype(np.float64)
+    solid = g.solid().reshape(32, 32, 64)
+    flux = (vel[..., 3] * vel[..., 0]).sum(axis=(0, 1))
+    assert np.allclose(flux, U * 32 * 32, rtol=2e-3)
+    out = vel[:, :, -1, 3][solid[:, :, -1] == 0]
+    assert abs(out.mean() - 1.0) < 1e-5
