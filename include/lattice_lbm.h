@@ -274,8 +274,8 @@ void *LBM_ParticlesDevice(LBMParticles *p);
 
 /* ---------------------------------------------------------------------
  * Batched sweeps: many independent grids advanced together, one kernel
- * launch per lattice step for the whole batch (CUDA-graph replays of
- * 32-step chunks), each grid with its own size, tau, operator,
+ * launch per lattice step for up to 64 grids (CUDA-graph replays of 32-step
+ * chunks), each grid with its own size, tau, operator,
  * Smagorinsky constant, geometry, periodic flag and inlet velocity.  The
  * reference runs one grid per process (main.c); a parameter sweep there is
  * many processes.  Every grid's populations are bit-identical to stepping
@@ -305,9 +305,8 @@ int LBM_BatchAutotune(LBMBatch *batch, int trialLaunches);
 int LBM_BatchGetTile(LBMBatch *batch, int index, int *tileX, int *tileY);
 int LBM_BatchSetTile(LBMBatch *batch, int index, int tileX);
 
-/* 256-cell tiles of one batched step (all grids), and the CUDA stream of
- * the batch.  A launch runs a fixed number of persistent blocks (a few per
- * SM) that stride over the tiles. */
+/* 256-cell tiles (thread blocks) of one batched step over all grids, and
+ * the CUDA stream of the batch. */
 long long LBM_BatchTilesPerStep(LBMBatch *batch);
 void *LBM_BatchGetStream(LBMBatch *batch);
 
@@ -392,6 +391,9 @@ void *LBM_WarmNetGetStream(LBMWarmNet *net);
  * in the network's normalised units, (target - shift) / scale.  Default
  * scale 1, shift 0. */
 int LBM_WarmNetSetOutputScaling(LBMWarmNet *net, const float *scale4, const float *shift4);
+/* Scale each training step's gradient by min(1, maxNorm / ||g||) (global
+ * L2 norm over all parameters); 0 turns clipping off (the default). */
+int LBM_WarmNetSetGradClip(LBMWarmNet *net, float maxNorm);
 /* Features / targets of a grid at 1/factor resolution into device arrays:
  * solid fraction of each factor^3 block with U and Re; block means of
  * ((rho - 1) / U^2, u / U) over fluid cells (solid cells count as rho = 1,

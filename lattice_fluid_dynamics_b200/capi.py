@@ -172,6 +172,7 @@ SIGNATURES = {
     "LBM_WarmNetTrainStepDevice": (C.c_int, [_vp, _vp, _vp, C.c_int, _f, _vp]),
     "LBM_WarmNetGetStream": (_vp, [_vp]),
     "LBM_WarmNetSetOutputScaling": (C.c_int, [_vp, _vp, _vp]),
+    "LBM_WarmNetSetGradClip": (C.c_int, [_vp, _f]),
     "LBM_WarmNetGridFeatures": (C.c_int, [_G, C.c_int, _f, _f, _vp]),
     "LBM_WarmNetGridTargets": (C.c_int, [_G, C.c_int, _f, _vp]),
     "LBM_InitializeFromWarmNet": (C.c_int, [_G, _vp, _f, _f, C.c_int]),
@@ -689,6 +690,9 @@ class WarmNet:
         sh = np.ascontiguousarray(shift, np.float32)
         self._check(self._L.LBM_WarmNetSetOutputScaling(self._n, _p(sc), _p(sh)),
                     "LBM_WarmNetSetOutputScaling")
+
+    def set_grad_clip(self, max_norm: float):
+        self._check(self._L.LBM_WarmNetSetGradClip(self._n, max_norm), "LBM_WarmNetSetGradClip")
 
     def train_step_device(self, feat_ptr: int, target_ptr: int, batch: int, lr: float) -> float:
         loss = C.c_double()

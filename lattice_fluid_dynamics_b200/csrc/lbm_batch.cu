@@ -1,14 +1,13 @@
 // Batched sweeps (LBM_Batch*): one kernel launch per lattice step advances
-// every grid of a batch.
+// up to 64 grids (larger batches take one launch per 64 grids).
 //
-// Each launch is k_step_batch over the concatenated tiles of all grids (a
-// persistent launch of a few blocks per SM striding over the tiles); the
-// per-grid arguments live in device memory (two arrays, one per buffer
-// parity, since consecutive steps swap source and destination), so a CUDA
-// graph of a 32-step chunk (A, B, A, B, ...) is independent of the
-// arguments' values and is re-used across runs as long as the batch's
-// launch shape is unchanged.  Before a run the batch stream waits for
-// every grid's stream; after it every grid's stream waits for the batch.
+// Each launch is k_step_batch over the concatenated tiles of its grids, the
+// per-grid arguments passed by value in the kernel parameter (two argument
+// sets, one per buffer parity, since consecutive steps swap source and
+// destination).  A CUDA graph of a 32-step chunk (A, B, A, B, ...) is
+// captured with those arguments and replayed while they stay the same.
+// Before a run the batch stream waits for every grid's stream; after it
+// every grid's stream waits for the batch.
 //
 // Grids leaving an explicit-f state (after LBM_InitializeFlow or a
 // geometry edit) first take their priming steps through their own
@@ -17,6 +16,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <new>
 #include <vector>
 
@@ -32,22 +32,15 @@ struct LBMBatch {
     std::vector<cudaEvent_t> grid_done;   // recorded on each grid's stream
     cudaEvent_t batch_done = nullptr;
     cudaStream_t stream = nullptr;
-    BatchEntry *entries_dev = nullptr;    // [2][count]
-    long long *starts_dev = nullptr;      // [count + 1]
-    // pinned staging of the arguments, double-buffered: run k fills half
-    // k % 2 after the copy out of it by run k - 2 has completed
-    BatchEntry *entries_host[2] = {nullptr, nullptr};  // [2][count] each
-    long long *starts_host[2] = {nullptr, nullptr};    // [count + 1] each
-    cudaEvent_t copied[2] = {nullptr, nullptr};
-    bool copy_pending[2] = {false, false};
-    int runs = 0;
-    long long blocks = 0;                 // tiles of one step (all grids)
-    int set = BATCH_SET_ALL;
-    int minb = 4;                         // resident blocks per SM the kernel is built for
-    unsigned persist = 0;                 // persistent blocks of a full launch
+    // launch groups: grid indices, ordered by operator, at most
+    // BATCH_LAUNCH_MAX per group; arguments of both buffer parities
+    std::vector<std::vector<int>> groups;
+    std::vector<BatchLaunchParams> params[2];
+    std::vector<int> sets;
+    // the CUDA graph of kChunk steps and the arguments it was captured with
     cudaGraphExec_t graph = nullptr;
-    long long graph_blocks = -1;
-    int graph_set = -1;
+    std::vector<BatchLaunchParams> graph_params[2];
+    std::vector<int> graph_sets;
 };
 
 namespace {
@@ -56,9 +49,9 @@ constexpr int kChunk = 32;  // even: buffer parity repeats after a replay
 
 GridImpl *impl(LBMGrid *g) { return static_cast<GridImpl *>(g->impl); }
 
-int choose_set(const LBMBatch &b) {
-    unsigned used = 0;
-    for (LBMGrid *g : b.grids) used |= 1u << (grid_op(g) * 2 + (g->useSmagorinsky == 1));
+int combo_of(LBMGrid *g) { return grid_op(g) * 2 + (g->useSmagorinsky == 1); }
+
+int set_of(unsigned used) {
     for (int s = BATCH_SET_BGK; s <= BATCH_SET_MRT_SMAG; s++)
         if (used == batch_set_mask(s)) return s;
     if ((used & ~batch_set_mask(BATCH_SET_BGK_REG)) == 0) return BATCH_SET_BGK_REG;
@@ -71,7 +64,7 @@ BatchEntry make_entry(LBMGrid *g, int lbx, const void *src, void *dst, const flo
     e.a.src = src;
     e.a.dst = dst;
     e.a.periodic = impl(g)->stream_periodic;
-    e.combo = grid_op(g) * 2 + (g->useSmagorinsky == 1);
+    e.combo = combo_of(g);
     e.lbx = lbx;
     const int bx = 1 << lbx, by = 256 >> lbx;
     e.tiles_x = (impl(g)->nx + bx - 1) / bx;
@@ -90,8 +83,25 @@ void drop_graph(LBMBatch &b) {
 
 bool fail(LBMGrid *any, cudaError_t e) { return !grid_ok(any, e); }
 
-unsigned persist_blocks(const LBMBatch &b) {
-    return (unsigned)(b.blocks < (long long)b.persist ? b.blocks : (long long)b.persist);
+// grids ordered by operator (so that most launch groups hold one operator
+// and get the specialised kernel), cut into groups of BATCH_LAUNCH_MAX
+void make_groups(LBMBatch &b) {
+    std::vector<int> order(b.count);
+    for (int i = 0; i < b.count; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return combo_of(b.grids[x]) < combo_of(b.grids[y]);
+    });
+    b.groups.clear();
+    for (int i = 0; i < b.count; i += BATCH_LAUNCH_MAX)
+        b.groups.emplace_back(order.begin() + i,
+                              order.begin() + std::min(b.count, i + BATCH_LAUNCH_MAX));
+}
+
+bool same_params(const std::vector<BatchLaunchParams> &a, const std::vector<BatchLaunchParams> &c) {
+    if (a.size() != c.size()) return false;
+    for (size_t i = 0; i < a.size(); i++)
+        if (memcmp(&a[i], &c[i], sizeof(BatchLaunchParams)) != 0) return false;
+    return true;
 }
 
 }  // namespace
@@ -117,31 +127,10 @@ LBMBatch *LBM_BatchCreate(LBMGrid **grids, int count) {
     b->grids.assign(grids, grids + count);
     b->lbx.assign(count, 5);  // 32 x 8 tiles, the single-grid default
     b->grid_done.assign(count, nullptr);
-    // persistent launch: minb blocks per SM (LBM_BATCH_MINB=3 trades
-    // occupancy for registers)
-    const char *menv = getenv("LBM_BATCH_MINB");
-    b->minb = (menv && atoi(menv) == 3) ? 3 : 4;
-    int dev = 0, sms = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        sms <= 0) {
-        delete b;
-        return nullptr;
-    }
-    b->persist = (unsigned)(sms * b->minb);
     bool good = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess;
     good = good && cudaEventCreateWithFlags(&b->batch_done, cudaEventDisableTiming) == cudaSuccess;
     for (int i = 0; good && i < count; i++)
         good = cudaEventCreateWithFlags(&b->grid_done[i], cudaEventDisableTiming) == cudaSuccess;
-    good = good && cudaMalloc(&b->entries_dev, sizeof(BatchEntry) * 2 * count) == cudaSuccess;
-    good = good && cudaMalloc(&b->starts_dev, sizeof(long long) * (count + 1)) == cudaSuccess;
-    for (int h = 0; h < 2; h++) {
-        good = good &&
-               cudaMallocHost(&b->entries_host[h], sizeof(BatchEntry) * 2 * count) == cudaSuccess;
-        good = good &&
-               cudaMallocHost(&b->starts_host[h], sizeof(long long) * (count + 1)) == cudaSuccess;
-        good = good && cudaEventCreateWithFlags(&b->copied[h], cudaEventDisableTiming) == cudaSuccess;
-    }
     if (!good) {
         LBM_BatchFree(b);
         return nullptr;
@@ -156,13 +145,6 @@ void LBM_BatchFree(LBMBatch *b) {
     for (cudaEvent_t e : b->grid_done)
         if (e) cudaEventDestroy(e);
     if (b->batch_done) cudaEventDestroy(b->batch_done);
-    cudaFree(b->entries_dev);
-    cudaFree(b->starts_dev);
-    for (int h = 0; h < 2; h++) {
-        cudaFreeHost(b->entries_host[h]);
-        cudaFreeHost(b->starts_host[h]);
-        if (b->copied[h]) cudaEventDestroy(b->copied[h]);
-    }
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -192,27 +174,34 @@ int LBM_BatchRun(LBMBatch *b, int nSteps, const float *inlet) {
     const int steps = nSteps - prime;
     if (steps == 0) return LBM_OK;
 
-    // arguments of both parities, tile offsets, launch shape
-    const int h = b->runs & 1;
-    if (b->copy_pending[h] && fail(g0, cudaEventSynchronize(b->copied[h]))) return LBM_ERR_CUDA;
-    b->copy_pending[h] = false;
-    BatchEntry *eh = b->entries_host[h];
-    long long *sh = b->starts_host[h];
-    long long total = 0;
-    for (int i = 0; i < n; i++) {
-        LBMGrid *g = b->grids[i];
-        GridImpl &I = *impl(g);
-        if (I.fbuf >= 0 || I.stream_periodic != g->periodicYZ) return LBM_ERR_CUDA;
-        const float *in = inlet + 3 * i;
-        eh[i] = make_entry(g, b->lbx[i], I.pop[I.gbuf], I.pop[1 - I.gbuf], in);
-        eh[n + i] = make_entry(g, b->lbx[i], I.pop[1 - I.gbuf], I.pop[I.gbuf], in);
-        sh[i] = total;
-        total += tiles_of(eh[i], I.nz);
+    // launch arguments of both parities for every group
+    make_groups(*b);
+    const size_t ng = b->groups.size();
+    for (int p = 0; p < 2; p++) b->params[p].assign(ng, BatchLaunchParams{});
+    b->sets.assign(ng, BATCH_SET_ALL);
+    for (size_t gi = 0; gi < ng; gi++) {
+        const std::vector<int> &grp = b->groups[gi];
+        unsigned used = 0;
+        long long total = 0;
+        for (size_t j = 0; j < grp.size(); j++) {
+            const int i = grp[j];
+            LBMGrid *g = b->grids[i];
+            GridImpl &I = *impl(g);
+            if (I.fbuf >= 0 || I.stream_periodic != g->periodicYZ) return LBM_ERR_CUDA;
+            const float *in = inlet + 3 * i;
+            b->params[0][gi].e[j] = make_entry(g, b->lbx[i], I.pop[I.gbuf], I.pop[1 - I.gbuf], in);
+            b->params[1][gi].e[j] = make_entry(g, b->lbx[i], I.pop[1 - I.gbuf], I.pop[I.gbuf], in);
+            b->params[0][gi].starts[j] = b->params[1][gi].starts[j] = (unsigned)total;
+            total += tiles_of(b->params[0][gi].e[j], I.nz);
+            used |= 1u << combo_of(g);
+        }
+        if (total > 0x7fffffffLL) return LBM_ERR_INVALID_ARGUMENT;
+        for (int p = 0; p < 2; p++) {
+            b->params[p][gi].starts[grp.size()] = (unsigned)total;
+            b->params[p][gi].count = (int)grp.size();
+        }
+        b->sets[gi] = set_of(used);
     }
-    sh[n] = total;
-    if (total > 0x7fffffffLL) return LBM_ERR_INVALID_ARGUMENT;
-    b->blocks = total;
-    b->set = choose_set(*b);
 
     // the batch waits for every grid's queued work
     for (int i = 0; i < n; i++) {
@@ -221,27 +210,22 @@ int LBM_BatchRun(LBMBatch *b, int nSteps, const float *inlet) {
         if (fail(b->grids[i], cudaStreamWaitEvent(b->stream, b->grid_done[i], 0)))
             return LBM_ERR_CUDA;
     }
-    if (fail(g0, cudaMemcpyAsync(b->entries_dev, eh, sizeof(BatchEntry) * 2 * n,
-                                 cudaMemcpyHostToDevice, b->stream)) ||
-        fail(g0, cudaMemcpyAsync(b->starts_dev, sh, sizeof(long long) * (n + 1),
-                                 cudaMemcpyHostToDevice, b->stream)) ||
-        fail(g0, cudaEventRecord(b->copied[h], b->stream)))
-        return LBM_ERR_CUDA;
-    b->copy_pending[h] = true;
-    b->runs++;
-
-    const BatchEntry *ea = b->entries_dev, *eb = b->entries_dev + n;
+    auto step = [&](int parity) {
+        for (size_t gi = 0; gi < ng; gi++)
+            if (fail(g0, launch_step_batch(b->storage, b->params[parity][gi], b->sets[gi],
+                                           b->stream)))
+                return false;
+        return true;
+    };
     int left = steps;
     if (left >= kChunk) {
-        if (!b->graph || b->graph_blocks != total || b->graph_set != b->set) {
+        if (!b->graph || b->graph_sets != b->sets || !same_params(b->graph_params[0], b->params[0]) ||
+            !same_params(b->graph_params[1], b->params[1])) {
             drop_graph(*b);
             cudaGraph_t graph = nullptr;
             bool good = !fail(g0, cudaStreamBeginCapture(b->stream,
                                                          cudaStreamCaptureModeThreadLocal));
-            for (int k = 0; good && k < kChunk; k++)
-                good = !fail(g0, launch_step_batch(b->storage, (k & 1) ? eb : ea, b->starts_dev,
-                                                   n, total, b->set, b->minb, persist_blocks(*b),
-                                                   b->stream));
+            for (int k = 0; good && k < kChunk; k++) good = step(k & 1);
             const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
             good = good && !fail(g0, e);
             cudaGraphExec_t exec = nullptr;
@@ -249,8 +233,9 @@ int LBM_BatchRun(LBMBatch *b, int nSteps, const float *inlet) {
             if (graph) cudaGraphDestroy(graph);
             if (!good) return LBM_ERR_CUDA;
             b->graph = exec;
-            b->graph_blocks = total;
-            b->graph_set = b->set;
+            b->graph_params[0] = b->params[0];
+            b->graph_params[1] = b->params[1];
+            b->graph_sets = b->sets;
         }
         while (left >= kChunk) {
             if (fail(g0, cudaGraphLaunch(b->graph, b->stream))) return LBM_ERR_CUDA;
@@ -258,9 +243,7 @@ int LBM_BatchRun(LBMBatch *b, int nSteps, const float *inlet) {
         }
     }
     for (int k = 0; k < left; k++)
-        if (fail(g0, launch_step_batch(b->storage, (k & 1) ? eb : ea, b->starts_dev, n, total,
-                                       b->set, b->minb, persist_blocks(*b), b->stream)))
-            return LBM_ERR_CUDA;
+        if (!step(k & 1)) return LBM_ERR_CUDA;
 
     // every grid's later work waits for the batch
     if (fail(g0, cudaEventRecord(b->batch_done, b->stream))) return LBM_ERR_CUDA;
@@ -281,18 +264,14 @@ int LBM_BatchAutotune(LBMBatch *b, int trialLaunches) {
     for (LBMGrid *g : b->grids) nmax = impl(g)->n > nmax ? impl(g)->n : nmax;
     void *scratch = nullptr;
     unsigned long long *guard = nullptr;
-    BatchEntry *ent = nullptr;
-    long long *st = nullptr;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
-    int rc = LBM_OK;
     bool good = !fail(g0, cudaMalloc(&scratch, (size_t)nmax * 19 * impl(g0)->elem)) &&
                 !fail(g0, cudaMalloc(&guard, sizeof(unsigned long long))) &&
-                !fail(g0, cudaMalloc(&ent, sizeof(BatchEntry))) &&
-                !fail(g0, cudaMalloc(&st, 2 * sizeof(long long))) &&
                 !fail(g0, cudaEventCreate(&t0)) && !fail(g0, cudaEventCreate(&t1));
     for (int i = 0; i < b->count; i++)
         good = good && !fail(b->grids[i], cudaStreamSynchronize(impl(b->grids[i])->stream));
     good = good && !fail(g0, cudaStreamSynchronize(b->stream));
+    BatchLaunchParams p{};
     for (int i = 0; good && i < b->count; i++) {
         LBMGrid *g = b->grids[i];
         GridImpl &I = *impl(g);
@@ -301,27 +280,17 @@ int LBM_BatchAutotune(LBMBatch *b, int trialLaunches) {
         float best = 1e30f;
         int best_lbx = b->lbx[i];
         for (int lbx = 5; good && lbx <= 8; lbx++) {
-            BatchEntry e = make_entry(g, lbx, src, scratch, in);
-            e.a.guard = guard;
-            const long long starts[2] = {0, tiles_of(e, I.nz)};
-            const unsigned bit = 1u << e.combo;
-            int set = BATCH_SET_ALL;
-            for (int s = BATCH_SET_BGK; s <= BATCH_SET_MRT_SMAG; s++)
-                if (bit == batch_set_mask(s)) set = s;
-            good = !fail(g, cudaMemcpyAsync(ent, &e, sizeof(e), cudaMemcpyHostToDevice,
-                                            b->stream)) &&
-                   !fail(g, cudaMemcpyAsync(st, starts, sizeof(starts), cudaMemcpyHostToDevice,
-                                            b->stream)) &&
-                   !fail(g, cudaStreamSynchronize(b->stream));
+            p.e[0] = make_entry(g, lbx, src, scratch, in);
+            p.e[0].a.guard = guard;
+            p.starts[0] = 0;
+            p.starts[1] = (unsigned)tiles_of(p.e[0], I.nz);
+            p.count = 1;
+            const int set = set_of(1u << p.e[0].combo);
             // one untimed launch, then the timed ones
-            const unsigned pb = (unsigned)(starts[1] < (long long)b->persist ? starts[1]
-                                                                               : b->persist);
-            good = good && !fail(g, launch_step_batch(b->storage, ent, st, 1, starts[1], set,
-                                                      b->minb, pb, b->stream));
-            good = good && !fail(g, cudaEventRecord(t0, b->stream));
+            good = !fail(g, launch_step_batch(b->storage, p, set, b->stream)) &&
+                   !fail(g, cudaEventRecord(t0, b->stream));
             for (int k = 0; good && k < trialLaunches; k++)
-                good = !fail(g, launch_step_batch(b->storage, ent, st, 1, starts[1], set,
-                                                  b->minb, pb, b->stream));
+                good = !fail(g, launch_step_batch(b->storage, p, set, b->stream));
             good = good && !fail(g, cudaEventRecord(t1, b->stream)) &&
                    !fail(g, cudaEventSynchronize(t1));
             float ms = 0;
@@ -337,14 +306,11 @@ int LBM_BatchAutotune(LBMBatch *b, int trialLaunches) {
             drop_graph(*b);
         }
     }
-    if (!good) rc = LBM_ERR_CUDA;
     if (t0) cudaEventDestroy(t0);
     if (t1) cudaEventDestroy(t1);
     cudaFree(scratch);
     cudaFree(guard);
-    cudaFree(ent);
-    cudaFree(st);
-    return rc;
+    return good ? LBM_OK : LBM_ERR_CUDA;
 }
 
 int LBM_BatchGetTile(LBMBatch *b, int index, int *tileX, int *tileY) {

@@ -26,10 +26,8 @@ cudaError_t launch_step(const GridImpl &g, const StepArgs &a, bool fused, int op
     LBM_DISPATCH(g.storage, step(g, a, fused, op, smag, s));
 }
 
-cudaError_t launch_step_batch(int storage, const BatchEntry *entries, const long long *starts,
-                              int count, long long tiles, int set, int minb, unsigned blocks,
-                              cudaStream_t s) {
-    LBM_DISPATCH(storage, batch(entries, starts, count, tiles, set, minb, blocks, s));
+cudaError_t launch_step_batch(int storage, const BatchLaunchParams &p, int set, cudaStream_t s) {
+    LBM_DISPATCH(storage, batch(p, set, s));
 }
 
 static StepArgs stream_args(const GridImpl &g, const void *src, void *dst, int periodic) {

@@ -129,11 +129,16 @@ bool grid_ok(LBMGrid *grid, cudaError_t e);
 int grid_init_from_device(LBMGrid *grid, const float *drho, const float *du);
 
 // lbm_step.cu
-// `tiles` tiles of all grids processed by `blocks` persistent blocks, the
-// kernel built for at least `minb` (3 or 4) resident blocks per SM
-cudaError_t launch_step_batch(int storage, const BatchEntry *entries_dev,
-                              const long long *starts_dev, int count, long long tiles, int set,
-                              int minb, unsigned blocks, cudaStream_t s);
+// Arguments of one batched launch, passed by value as a kernel parameter
+// (constant bank): up to BATCH_LAUNCH_MAX grids, tile t belonging to grid g
+// with starts[g] <= t < starts[g + 1].
+constexpr int BATCH_LAUNCH_MAX = 64;
+struct BatchLaunchParams {
+    BatchEntry e[BATCH_LAUNCH_MAX];
+    unsigned starts[BATCH_LAUNCH_MAX + 1];
+    int count;
+};
+cudaError_t launch_step_batch(int storage, const BatchLaunchParams &p, int set, cudaStream_t s);
 cudaError_t launch_step(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
                         bool fast_arith, cudaStream_t s);
 namespace fast {

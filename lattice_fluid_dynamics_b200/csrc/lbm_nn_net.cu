@@ -197,12 +197,27 @@ __global__ void k_bias_grad(const __nv_bfloat16 *__restrict__ g, int nt, long lo
     if (threadIdx.x == 0) db[c] = (float)part[0];
 }
 
+// sum of squares of the gradient (for global-norm clipping)
+__global__ void k_sqnorm(const float *__restrict__ g, long long n, double *__restrict__ out) {
+    double acc = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        acc += (double)g[i] * g[i];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+// Adam; with clip > 0 the gradient is scaled by min(1, clip / ||g||)
 __global__ void k_adam(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ mo,
                        float *__restrict__ ve, long long n, float lr_t, float b1, float b2,
-                       float eps) {
+                       float eps, float clip, const double *__restrict__ sq) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float gi = g[i];
+    float gi = g[i];
+    if (clip > 0.f) {
+        const double norm = sqrt(*sq);
+        if (norm > clip) gi *= (float)(clip / norm);
+    }
     const float mi = b1 * mo[i] + (1.f - b1) * gi;
     const float vi = b2 * ve[i] + (1.f - b2) * gi * gi;
     mo[i] = mi;
@@ -398,6 +413,8 @@ struct LBMWarmNet {
     double *loss = nullptr;
     int error = 0;
     OutScale out_scale = {{1.f, 1.f, 1.f, 1.f}, {0.f, 0.f, 0.f, 0.f}};
+    float clip = 0.f;
+    double *sq = nullptr;
 
     template <class T>
     T *alloc(long long n) {
@@ -762,6 +779,7 @@ LBMWarmNet *LBM_WarmNetCreate(int nx, int ny, int nz, int maxBatch, unsigned see
     n->target = n->alloc<float>(m1 * 4);
     n->pred32 = n->alloc<float>(m1 * 4);
     n->loss = n->alloc<double>(1);
+    n->sq = n->alloc<double>(1);
     if (n->error) {
         LBM_WarmNetFree(n);
         return nullptr;
@@ -865,8 +883,12 @@ int LBM_WarmNetTrainStepDevice(LBMWarmNet *n, const float *features, const float
     const float b1 = 0.9f, b2 = 0.999f;
     const float lr_t = lr * sqrtf(1.f - powf(b2, (float)n->adam_t)) /
                        (1.f - powf(b1, (float)n->adam_t));
+    if (n->clip > 0.f) {
+        if (!ok(n, cudaMemsetAsync(n->sq, 0, sizeof(double), n->stream))) return LBM_ERR_CUDA;
+        k_sqnorm<<<148 * 4, 256, 0, n->stream>>>(n->grad, n->P, n->sq);
+    }
     k_adam<<<nblk(n->P), 256, 0, n->stream>>>(n->params, n->grad, n->am, n->av, n->P, lr_t, b1, b2,
-                                              1e-8f);
+                                              1e-8f, n->clip, n->sq);
     if (!ok(n, cudaGetLastError())) return LBM_ERR_CUDA;
     n->packed = false;
     if (!pack(n)) return LBM_ERR_CUDA;
@@ -891,6 +913,12 @@ int LBM_WarmNetTrainStep(LBMWarmNet *n, const float *features, const float *targ
 }
 
 void *LBM_WarmNetGetStream(LBMWarmNet *n) { return n ? (void *)n->stream : nullptr; }
+
+int LBM_WarmNetSetGradClip(LBMWarmNet *n, float maxNorm) {
+    if (!n || !(maxNorm >= 0.f)) return LBM_ERR_INVALID_ARGUMENT;
+    n->clip = maxNorm;
+    return LBM_OK;
+}
 
 int LBM_WarmNetSetOutputScaling(LBMWarmNet *n, const float *scale4, const float *shift4) {
     if (!n || !scale4 || !shift4) return LBM_ERR_INVALID_ARGUMENT;

@@ -254,52 +254,38 @@ __global__ void __launch_bounds__(256, MINB) k_step(const StepArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Batched step: one launch advances every grid of a batch by one fused step.
-// The work is the concatenation of every grid's tiles (tile t of the batch
-// belongs to the grid g with starts[g] <= t < starts[g + 1]).  The launch is
-// persistent -- a fixed number of 256-thread blocks, each striding over the
-// tiles by the launch size, so the blocks resident at any moment work on
-// neighbouring tiles -- and a block keeps the StepArgs of its current grid
-// in shared memory, reloading them only when its tiles cross into the next
-// grid.  The per-cell code is k_step's, so every grid's result is
-// bit-identical to a solo step.  Each grid has its own tile shape
-// (BatchEntry::lbx).
-template <class S, int SET, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_step_batch(const BatchEntry *__restrict__ entries,
-                                                           const long long *__restrict__ starts,
-                                                           int count, long long total_tiles) {
-    __shared__ BatchEntry e;
-    int cur = 0;
-    long long lo = 0, hi = -1;  // tile range of the grid held in `e`
-    for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x) {
-        if (t >= hi) {  // uniform across the block
-            while (cur + 1 < count && __ldg(starts + cur + 1) <= t) cur++;
-            __syncthreads();  // every thread is done with the previous grid
-            const int *src = reinterpret_cast<const int *>(entries + cur);
-            int *dst = reinterpret_cast<int *>(&e);
-            for (int k = threadIdx.x; k < (int)(sizeof(BatchEntry) / sizeof(int)); k += 256)
-                dst[k] = __ldg(src + k);
-            __syncthreads();
-            lo = __ldg(starts + cur);
-            hi = __ldg(starts + cur + 1);
-        }
-        const long long local = t - lo;
-        const int tx = (int)(local % e.tiles_x);
-        const long long rest = local / e.tiles_x;
-        const int ty = (int)(rest % e.tiles_y);
-        const int z = (int)(rest / e.tiles_y);
-        const int bx = 1 << e.lbx;
-        const int x = tx * bx + (threadIdx.x & (bx - 1));
-        const int y = ty * (256 >> e.lbx) + (threadIdx.x >> e.lbx);
-        constexpr unsigned M = batch_set_mask(SET);
-        switch (e.combo) {
-            case 0: if constexpr ((M & 1u) != 0) step_cells<S, OP_BGK, false, true, 1>(e.a, x, y, z); break;
-            case 1: if constexpr ((M & 2u) != 0) step_cells<S, OP_BGK, true, true, 1>(e.a, x, y, z); break;
-            case 2: if constexpr ((M & 4u) != 0) step_cells<S, OP_REG, false, true, 1>(e.a, x, y, z); break;
-            case 3: if constexpr ((M & 8u) != 0) step_cells<S, OP_REG, true, true, 1>(e.a, x, y, z); break;
-            case 4: if constexpr ((M & 16u) != 0) step_cells<S, OP_MRT, false, true, 1>(e.a, x, y, z); break;
-            default: if constexpr ((M & 32u) != 0) step_cells<S, OP_MRT, true, true, 1>(e.a, x, y, z); break;
-        }
+// Batched step: one launch advances up to BATCH_LAUNCH_MAX grids by one
+// fused step.  One 256-thread block per tile of the concatenated tiles of
+// all grids; the block finds its grid by binary search over the tile
+// offsets and reads that grid's StepArgs straight from the kernel parameter
+// (constant bank, uniform across the block).  The per-cell code is
+// k_step's, so every grid's result is bit-identical to a solo step.  Each
+// grid has its own tile shape (BatchEntry::lbx).
+template <class S, int SET>
+__global__ void __launch_bounds__(256, 4) k_step_batch(const __grid_constant__ BatchLaunchParams p) {
+    const unsigned b = blockIdx.x;
+    int lo = 0, hi = p.count - 1;  // largest grid index with starts <= b
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (p.starts[mid] <= b) lo = mid; else hi = mid - 1;
+    }
+    const BatchEntry &e = p.e[lo];
+    const unsigned local = b - p.starts[lo];
+    const unsigned tx = local % (unsigned)e.tiles_x;
+    const unsigned rest = local / (unsigned)e.tiles_x;
+    const int ty = (int)(rest % (unsigned)e.tiles_y);
+    const int z = (int)(rest / (unsigned)e.tiles_y);
+    const int bx = 1 << e.lbx;
+    const int x = (int)tx * bx + (threadIdx.x & (bx - 1));
+    const int y = ty * (256 >> e.lbx) + (threadIdx.x >> e.lbx);
+    constexpr unsigned M = batch_set_mask(SET);
+    switch (e.combo) {
+        case 0: if constexpr ((M & 1u) != 0) step_cells<S, OP_BGK, false, true, 1>(e.a, x, y, z); break;
+        case 1: if constexpr ((M & 2u) != 0) step_cells<S, OP_BGK, true, true, 1>(e.a, x, y, z); break;
+        case 2: if constexpr ((M & 4u) != 0) step_cells<S, OP_REG, false, true, 1>(e.a, x, y, z); break;
+        case 3: if constexpr ((M & 8u) != 0) step_cells<S, OP_REG, true, true, 1>(e.a, x, y, z); break;
+        case 4: if constexpr ((M & 16u) != 0) step_cells<S, OP_MRT, false, true, 1>(e.a, x, y, z); break;
+        default: if constexpr ((M & 32u) != 0) step_cells<S, OP_MRT, true, true, 1>(e.a, x, y, z); break;
     }
 }
 
@@ -516,29 +502,18 @@ struct StepLaunch {
         return cudaGetLastError();
     }
 
-    template <int SET>
-    static void batch_go(const BatchEntry *entries, const long long *starts, int count,
-                         long long tiles, int minb, unsigned blocks, cudaStream_t s) {
-        if (minb == 3)
-            k_step_batch<S, SET, 3><<<blocks, 256, 0, s>>>(entries, starts, count, tiles);
-        else
-            k_step_batch<S, SET, 4><<<blocks, 256, 0, s>>>(entries, starts, count, tiles);
-    }
-
-    // `blocks` persistent blocks over `tiles` tiles
-    static cudaError_t batch(const BatchEntry *entries, const long long *starts, int count,
-                             long long tiles, int set, int minb, unsigned blocks,
-                             cudaStream_t s) {
-        if (tiles <= 0 || blocks == 0) return cudaErrorInvalidValue;
+    static cudaError_t batch(const BatchLaunchParams &p, int set, cudaStream_t s) {
+        const unsigned tiles = p.starts[p.count];
+        if (p.count <= 0 || p.count > BATCH_LAUNCH_MAX || tiles == 0) return cudaErrorInvalidValue;
         switch (set) {
-            case BATCH_SET_BGK: batch_go<BATCH_SET_BGK>(entries, starts, count, tiles, minb, blocks, s); break;
-            case BATCH_SET_BGK_SMAG: batch_go<BATCH_SET_BGK_SMAG>(entries, starts, count, tiles, minb, blocks, s); break;
-            case BATCH_SET_REG: batch_go<BATCH_SET_REG>(entries, starts, count, tiles, minb, blocks, s); break;
-            case BATCH_SET_REG_SMAG: batch_go<BATCH_SET_REG_SMAG>(entries, starts, count, tiles, minb, blocks, s); break;
-            case BATCH_SET_MRT: batch_go<BATCH_SET_MRT>(entries, starts, count, tiles, minb, blocks, s); break;
-            case BATCH_SET_MRT_SMAG: batch_go<BATCH_SET_MRT_SMAG>(entries, starts, count, tiles, minb, blocks, s); break;
-            case BATCH_SET_BGK_REG: batch_go<BATCH_SET_BGK_REG>(entries, starts, count, tiles, minb, blocks, s); break;
-            default: batch_go<BATCH_SET_ALL>(entries, starts, count, tiles, minb, blocks, s); break;
+            case BATCH_SET_BGK: k_step_batch<S, BATCH_SET_BGK><<<tiles, 256, 0, s>>>(p); break;
+            case BATCH_SET_BGK_SMAG: k_step_batch<S, BATCH_SET_BGK_SMAG><<<tiles, 256, 0, s>>>(p); break;
+            case BATCH_SET_REG: k_step_batch<S, BATCH_SET_REG><<<tiles, 256, 0, s>>>(p); break;
+            case BATCH_SET_REG_SMAG: k_step_batch<S, BATCH_SET_REG_SMAG><<<tiles, 256, 0, s>>>(p); break;
+            case BATCH_SET_MRT: k_step_batch<S, BATCH_SET_MRT><<<tiles, 256, 0, s>>>(p); break;
+            case BATCH_SET_MRT_SMAG: k_step_batch<S, BATCH_SET_MRT_SMAG><<<tiles, 256, 0, s>>>(p); break;
+            case BATCH_SET_BGK_REG: k_step_batch<S, BATCH_SET_BGK_REG><<<tiles, 256, 0, s>>>(p); break;
+            default: k_step_batch<S, BATCH_SET_ALL><<<tiles, 256, 0, s>>>(p); break;
         }
         return cudaGetLastError();
     }

@@ -137,11 +137,16 @@ def make_dataset(count: int, seed: int, dims=(128, 64, 64), steps: int = 6000,
 # training
 
 def train(net: capi.WarmNet, feats, tgts, epochs: int, batch: int, lr: float, seed: int = 0,
-          val=None):
+          val=None, warmup: int = 200, clip: float = 1.0):
+    """Adam with linear warm-up then cosine decay and global gradient-norm
+    clipping; with a validation set, the weights of the best validation loss
+    are kept."""
     import torch
     n = feats.shape[0]
     rng = np.random.default_rng(seed)
     steps = epochs * (n // batch)
+    net.set_grad_clip(clip)
+    best, best_params = math.inf, None
     history, t0, s = [], time.perf_counter(), 0
     fb = torch.empty((batch,) + tuple(feats.shape[1:]), dtype=torch.float32, device="cuda")
     tb = torch.empty((batch,) + tuple(tgts.shape[1:]), dtype=torch.float32, device="cuda")
@@ -153,13 +158,17 @@ def train(net: capi.WarmNet, feats, tgts, epochs: int, batch: int, lr: float, se
             torch.index_select(feats, 0, idx, out=fb)
             torch.index_select(tgts, 0, idx, out=tb)
             torch.cuda.synchronize()
-            lr_s = lr * 0.5 * (1 + math.cos(math.pi * s / steps))  # cosine decay
+            lr_s = lr * min(1.0, (s + 1) / warmup) * 0.5 * (1 + math.cos(math.pi * s / steps))
             losses.append(net.train_step_device(fb.data_ptr(), tb.data_ptr(), batch, lr_s))
             s += 1
         rec = {"epoch": ep, "train_loss": float(np.mean(losses))}
         if val is not None:
             rec["val_loss"] = evaluate_loss(net, *val)
+            if rec["val_loss"] < best:
+                best, best_params = rec["val_loss"], net.params()
         history.append(rec)
+    if best_params is not None:
+        net.set_params(best_params)
     return history, time.perf_counter() - t0
 
 
@@ -327,7 +336,7 @@ def main(argv=None) -> int:
     ap.add_argument("--snapshot-steps", type=int, default=6000)
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--batch", type=int, default=8)
-    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr", type=float, default=3e-4)
     ap.add_argument("--grid", default="256x128x128")
     ap.add_argument("--cold-steps", type=int, default=30000)
     ap.add_argument("--sample", type=int, default=50)
@@ -383,7 +392,7 @@ def _train_from_snapshots(net, a, half, res):
                            "min": t.min(0).values.tolist(), "max": t.max(0).values.tolist()}
     # every output channel in units of its spread over the training set
     mean, std = t.mean(0), t.std(0).clamp_min(1e-6)
-    tgts = (tgts - mean) / std
+    tgts = ((tgts - mean) / std).clamp(-8.0, 8.0)  # rare stagnation-point outliers
     net.set_output_scaling(std.cpu().numpy(), mean.cpu().numpy())
     res["output_scaling"] = {"scale": std.tolist(), "shift": mean.tolist()}
     hist, tsec = train(net, feats[:ntr], tgts[:ntr], a.epochs, a.batch, a.lr,

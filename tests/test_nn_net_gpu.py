@@ -83,6 +83,7 @@ def test_training_reduces_loss(solver):
     fluid = 1.0 - feats[:, 0]
     target = np.stack([0.5 * fluid, fluid * (1 + feats[:, 1] * 5), 0.1 * fluid,
                        np.zeros(m)], 1).astype(np.float32)
+    net.set_grad_clip(5.0)
     losses = [net.train_step(feats, target, 3e-3) for _ in range(150)]
     assert all(np.isfinite(losses))
     assert losses[-1] < 0.1 * losses[0], (losses[0], losses[-1])
