@@ -274,8 +274,8 @@ void *LBM_ParticlesDevice(LBMParticles *p);
 
 /* ---------------------------------------------------------------------
  * Batched sweeps: many independent grids advanced together, one kernel
- * launch per lattice step for up to 64 grids (CUDA-graph replays of 32-step
- * chunks), each grid with its own size, tau, operator,
+ * launch per lattice step for up to 64 grids of one collision operator
+ * (CUDA-graph replays of 32-step chunks), each grid with its own size, tau, operator,
  * Smagorinsky constant, geometry, periodic flag and inlet velocity.  The
  * reference runs one grid per process (main.c); a parameter sweep there is
  * many processes.  Every grid's populations are bit-identical to stepping
@@ -305,8 +305,8 @@ int LBM_BatchAutotune(LBMBatch *batch, int trialLaunches);
 int LBM_BatchGetTile(LBMBatch *batch, int index, int *tileX, int *tileY);
 int LBM_BatchSetTile(LBMBatch *batch, int index, int tileX);
 
-/* 256-cell tiles (thread blocks) of one batched step over all grids, and
- * the CUDA stream of the batch. */
+/* 256-cell tiles of one batched step over all grids, and the CUDA stream of
+ * the batch. */
 long long LBM_BatchTilesPerStep(LBMBatch *batch);
 void *LBM_BatchGetStream(LBMBatch *batch);
 

@@ -1,5 +1,6 @@
 // Batched sweeps (LBM_Batch*): one kernel launch per lattice step advances
-// up to 64 grids (larger batches take one launch per 64 grids).
+// up to 64 grids of one operator (a batch takes one launch per operator and
+// per 64 grids).
 //
 // Each launch is k_step_batch over the concatenated tiles of its grids, the
 // per-grid arguments passed by value in the kernel parameter (two argument
@@ -72,7 +73,10 @@ BatchEntry make_entry(LBMGrid *g, int lbx, const void *src, void *dst, const flo
     return e;
 }
 
-long long tiles_of(const BatchEntry &e, int nz) { return (long long)e.tiles_x * e.tiles_y * nz; }
+// work units (tile columns of BATCH_ZB z-planes) of one grid
+long long units_of(const BatchEntry &e, int nz) {
+    return (long long)e.tiles_x * e.tiles_y * ((nz + BATCH_ZB - 1) / BATCH_ZB);
+}
 
 void drop_graph(LBMBatch &b) {
     if (b.graph) {
@@ -83,18 +87,18 @@ void drop_graph(LBMBatch &b) {
 
 bool fail(LBMGrid *any, cudaError_t e) { return !grid_ok(any, e); }
 
-// grids ordered by operator (so that most launch groups hold one operator
-// and get the specialised kernel), cut into groups of BATCH_LAUNCH_MAX
+// one launch group per operator (each gets the kernel specialised to it),
+// cut into groups of at most BATCH_LAUNCH_MAX grids
 void make_groups(LBMBatch &b) {
-    std::vector<int> order(b.count);
-    for (int i = 0; i < b.count; i++) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-        return combo_of(b.grids[x]) < combo_of(b.grids[y]);
-    });
     b.groups.clear();
-    for (int i = 0; i < b.count; i += BATCH_LAUNCH_MAX)
-        b.groups.emplace_back(order.begin() + i,
-                              order.begin() + std::min(b.count, i + BATCH_LAUNCH_MAX));
+    for (int c = 0; c < 6; c++) {
+        std::vector<int> grp;
+        for (int i = 0; i < b.count; i++)
+            if (combo_of(b.grids[i]) == c) grp.push_back(i);
+        for (size_t k = 0; k < grp.size(); k += BATCH_LAUNCH_MAX)
+            b.groups.emplace_back(grp.begin() + k,
+                                  grp.begin() + std::min(grp.size(), k + BATCH_LAUNCH_MAX));
+    }
 }
 
 bool same_params(const std::vector<BatchLaunchParams> &a, const std::vector<BatchLaunchParams> &c) {
@@ -192,7 +196,7 @@ int LBM_BatchRun(LBMBatch *b, int nSteps, const float *inlet) {
             b->params[0][gi].e[j] = make_entry(g, b->lbx[i], I.pop[I.gbuf], I.pop[1 - I.gbuf], in);
             b->params[1][gi].e[j] = make_entry(g, b->lbx[i], I.pop[1 - I.gbuf], I.pop[I.gbuf], in);
             b->params[0][gi].starts[j] = b->params[1][gi].starts[j] = (unsigned)total;
-            total += tiles_of(b->params[0][gi].e[j], I.nz);
+            total += units_of(b->params[0][gi].e[j], I.nz);
             used |= 1u << combo_of(g);
         }
         if (total > 0x7fffffffLL) return LBM_ERR_INVALID_ARGUMENT;
@@ -283,7 +287,7 @@ int LBM_BatchAutotune(LBMBatch *b, int trialLaunches) {
             p.e[0] = make_entry(g, lbx, src, scratch, in);
             p.e[0].a.guard = guard;
             p.starts[0] = 0;
-            p.starts[1] = (unsigned)tiles_of(p.e[0], I.nz);
+            p.starts[1] = (unsigned)units_of(p.e[0], I.nz);
             p.count = 1;
             const int set = set_of(1u << p.e[0].combo);
             // one untimed launch, then the timed ones

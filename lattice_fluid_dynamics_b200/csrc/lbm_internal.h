@@ -130,9 +130,11 @@ int grid_init_from_device(LBMGrid *grid, const float *drho, const float *du);
 
 // lbm_step.cu
 // Arguments of one batched launch, passed by value as a kernel parameter
-// (constant bank): up to BATCH_LAUNCH_MAX grids, tile t belonging to grid g
-// with starts[g] <= t < starts[g + 1].
+// (constant bank): up to BATCH_LAUNCH_MAX grids, work unit t (a column of
+// BATCH_ZB z-planes of one tile) belonging to grid g with starts[g] <= t <
+// starts[g + 1].
 constexpr int BATCH_LAUNCH_MAX = 64;
+constexpr int BATCH_ZB = 1;  // z-planes of one tile per thread block
 struct BatchLaunchParams {
     BatchEntry e[BATCH_LAUNCH_MAX];
     unsigned starts[BATCH_LAUNCH_MAX + 1];

@@ -255,12 +255,13 @@ __global__ void __launch_bounds__(256, MINB) k_step(const StepArgs a) {
 
 // ---------------------------------------------------------------------------
 // Batched step: one launch advances up to BATCH_LAUNCH_MAX grids by one
-// fused step.  One 256-thread block per tile of the concatenated tiles of
-// all grids; the block finds its grid by binary search over the tile
-// offsets and reads that grid's StepArgs straight from the kernel parameter
-// (constant bank, uniform across the block).  The per-cell code is
-// k_step's, so every grid's result is bit-identical to a solo step.  Each
-// grid has its own tile shape (BatchEntry::lbx).
+// fused step.  Work unit: a column of up to BATCH_ZB consecutive z-planes of
+// one 256-cell tile, one 256-thread block per unit; the block finds its grid
+// by binary search over the unit offsets and reads that grid's StepArgs
+// straight from the kernel parameter (constant bank, uniform across the
+// block), then walks its z-planes.  The per-cell code is k_step's, so every
+// grid's result is bit-identical to a solo step.  Each grid has its own tile
+// shape (BatchEntry::lbx).
 template <class S, int SET>
 __global__ void __launch_bounds__(256, 4) k_step_batch(const __grid_constant__ BatchLaunchParams p) {
     const unsigned b = blockIdx.x;
@@ -274,18 +275,28 @@ __global__ void __launch_bounds__(256, 4) k_step_batch(const __grid_constant__ B
     const unsigned tx = local % (unsigned)e.tiles_x;
     const unsigned rest = local / (unsigned)e.tiles_x;
     const int ty = (int)(rest % (unsigned)e.tiles_y);
-    const int z = (int)(rest / (unsigned)e.tiles_y);
+    const int z0 = (int)(rest / (unsigned)e.tiles_y) * BATCH_ZB;
+    const int z1 = min(z0 + BATCH_ZB, e.a.nz);
     const int bx = 1 << e.lbx;
     const int x = (int)tx * bx + (threadIdx.x & (bx - 1));
     const int y = ty * (256 >> e.lbx) + (threadIdx.x >> e.lbx);
     constexpr unsigned M = batch_set_mask(SET);
-    switch (e.combo) {
-        case 0: if constexpr ((M & 1u) != 0) step_cells<S, OP_BGK, false, true, 1>(e.a, x, y, z); break;
-        case 1: if constexpr ((M & 2u) != 0) step_cells<S, OP_BGK, true, true, 1>(e.a, x, y, z); break;
-        case 2: if constexpr ((M & 4u) != 0) step_cells<S, OP_REG, false, true, 1>(e.a, x, y, z); break;
-        case 3: if constexpr ((M & 8u) != 0) step_cells<S, OP_REG, true, true, 1>(e.a, x, y, z); break;
-        case 4: if constexpr ((M & 16u) != 0) step_cells<S, OP_MRT, false, true, 1>(e.a, x, y, z); break;
-        default: if constexpr ((M & 32u) != 0) step_cells<S, OP_MRT, true, true, 1>(e.a, x, y, z); break;
+    auto cells = [&](int z) {
+        switch (e.combo) {
+            case 0: if constexpr ((M & 1u) != 0) step_cells<S, OP_BGK, false, true, 1>(e.a, x, y, z); break;
+            case 1: if constexpr ((M & 2u) != 0) step_cells<S, OP_BGK, true, true, 1>(e.a, x, y, z); break;
+            case 2: if constexpr ((M & 4u) != 0) step_cells<S, OP_REG, false, true, 1>(e.a, x, y, z); break;
+            case 3: if constexpr ((M & 8u) != 0) step_cells<S, OP_REG, true, true, 1>(e.a, x, y, z); break;
+            case 4: if constexpr ((M & 16u) != 0) step_cells<S, OP_MRT, false, true, 1>(e.a, x, y, z); break;
+            default: if constexpr ((M & 32u) != 0) step_cells<S, OP_MRT, true, true, 1>(e.a, x, y, z); break;
+        }
+    };
+    if constexpr (BATCH_ZB == 1) {
+        (void)z1;
+        cells(z0);
+    } else {
+#pragma unroll 1
+        for (int z = z0; z < z1; z++) cells(z);
     }
 }
 
