@@ -89,11 +89,14 @@ def random_union(seed: int, index: int) -> dict:
 
 
 def make_grid(shape: dict, dims, storage: str = "fp32") -> capi.Grid:
+    """storage: fp32 | fp16 | bf16 | fp64, with "-fast" for LBM_ARITH_FAST."""
     nx, ny, nz = dims
     L_cells = shape["length_world"] * nx / 8.0
     _, nu, _, _ = capi.reynolds_to_tau(shape["U"], L_cells, shape["Re"])
-    g = capi.Grid(nx, ny, nz, nu, storage=storage)
-    g.set(useRegularized=1, periodicYZ=1)
+    fast = storage.endswith("-fast")
+    g = capi.Grid(nx, ny, nz, nu, storage=storage.replace("-fast", ""))
+    g.set(useRegularized=1, periodicYZ=1,
+          arithmetic=capi.LBM_ARITH_FAST if fast else capi.LBM_ARITH_EXACT)
     g.set_solid_mesh(shape["triangles"], shape["bbox"])
     return g
 
@@ -225,6 +228,9 @@ VARIANTS = {
     "warm_fp32": ("fp32", "warm"),
     "warmu_fp16": ("fp16", "warm_velocity"),
     "warmc_fp16": ("fp16", "warm_flux"),
+    # FP16 storage with the contracted / approximate-division step kernels:
+    # the storage rounding (~1e-3) dominates the arithmetic's
+    "warmc_fp16fast": ("fp16-fast", "warm_flux"),
     "warmc_fp32": ("fp32", "warm_flux"),
     "cold_fp16": ("fp16", "cold"),
 }
@@ -327,6 +333,47 @@ def summarize(rows, variant="warm_fp16"):
     return out
 
 
+def bench_train(steps: int, batch: int = 8, dims=(64, 32, 32)) -> dict:
+    """Time `steps` training steps (forward + backward + Adam) on synthetic
+    data at the network resolution `dims` (x, y, z) with CUDA events on the
+    network's stream; algorithmic FLOPs = 3 x forward convolution FLOPs."""
+    import torch
+    nx, ny, nz = dims
+    net = capi.WarmNet(nx, ny, nz, max_batch=batch, seed=1)
+    rng = np.random.default_rng(0)
+    m = batch * nx * ny * nz
+    feats = torch.from_numpy(np.stack([(rng.random(m) < 0.1), np.full(m, 0.05),
+                                       np.full(m, 300.0)], 1).astype(np.float32)).cuda()
+    tgt = torch.from_numpy(rng.normal(size=(m, 4)).astype(np.float32)).cuda()
+    for _ in range(3):
+        net.train_step_device(feats.data_ptr(), tgt.data_ptr(), batch, 1e-4)
+    stream = torch.cuda.ExternalStream(capi.load().LBM_WarmNetGetStream(net.handle))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        net.train_step_device(feats.data_ptr(), tgt.data_ptr(), batch, 1e-4)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    flops = 3 * batch * forward_flops(nx, ny, nz)
+    return {"dims": [nx, ny, nz], "batch": batch, "ms_per_step": ms,
+            "gflop_per_step": flops / 1e9, "tflops": flops / (ms * 1e-3) / 1e12}
+
+
+# (cin, cout, level) of the 16 convolutions
+_LAYERS = [(8, 16, 0), (16, 16, 0), (16, 32, 1), (32, 32, 1), (32, 64, 2), (64, 64, 2),
+           (64, 128, 3), (128, 128, 3), (128, 128, 3), (192, 64, 2), (64, 64, 2), (96, 32, 1),
+           (32, 32, 1), (48, 16, 0), (16, 16, 0), (16, 4, 0)]
+
+
+def forward_flops(nx: int, ny: int, nz: int) -> float:
+    """Algorithmic FLOPs of one forward pass per sample: 2 per multiply-add
+    of every 3x3x3 convolution (real channels)."""
+    vox = nx * ny * nz
+    return float(sum(2 * 27 * ci * co * (vox >> (3 * lv)) for ci, co, lv in _LAYERS))
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--train", type=int, default=2000)
@@ -344,8 +391,13 @@ def main(argv=None) -> int:
                     help="comma list of " + ",".join(VARIANTS))
     ap.add_argument("--params", default="", help="trained parameters (.npy): skip training")
     ap.add_argument("--scaling", default="", help="results .json holding the output scaling")
+    ap.add_argument("--bench-train", type=int, default=0,
+                    help="only time this many training steps on synthetic data")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
+    if a.bench_train:
+        print(json.dumps(bench_train(a.bench_train, a.batch)))
+        return 0
     full = tuple(int(v) for v in a.grid.split("x"))
     half = tuple(v // 2 for v in full)
     res = {"grid": list(full), "snapshot_grid": list(half), "train": a.train, "seed": a.seed}
