@@ -273,9 +273,8 @@ int LBM_ParticlesLoad(LBMParticles *p, const LBMParticle *host);
 void *LBM_ParticlesDevice(LBMParticles *p);
 
 /* ---------------------------------------------------------------------
- * Batched sweeps: many independent grids advanced together, one kernel
- * launch per lattice step for up to 64 grids of one collision operator
- * (CUDA-graph replays of 32-step chunks), each grid with its own size, tau, operator,
+ * Batched sweeps: many independent grids advanced together, replayed from
+ * a CUDA graph of 32 steps (one graph launch per 32 steps of the batch), each grid with its own size, tau, operator,
  * Smagorinsky constant, geometry, periodic flag and inlet velocity.  The
  * reference runs one grid per process (main.c); a parameter sweep there is
  * many processes.  Every grid's populations are bit-identical to stepping
@@ -296,14 +295,25 @@ void LBM_BatchFree(LBMBatch *batch);
 int LBM_BatchRun(LBMBatch *batch, int nSteps, const float *inlet);
 
 /* Choose each grid's tile width (32, 64, 128 or 256 cells along x; 256 /
- * width rows) by timing `trialLaunches` launches of each candidate on that
- * grid alone, writing into scratch memory (the grids' state is untouched).
- * Returns LBM_OK or an LBM_ERR_* code. */
+ * width rows) for each schedule by timing `trialLaunches` launches of each
+ * candidate on that grid alone, then the schedule (below) by timing a whole
+ * step of each.  The timed launches write only the buffer the grids' next
+ * step overwrites, after materialising the velocity field, so the grids'
+ * state is untouched.  Returns LBM_OK or an LBM_ERR_* code. */
 int LBM_BatchAutotune(LBMBatch *batch, int trialLaunches);
 
 /* Tile shape of grid `index` (tileX cells along x by tileY rows). */
 int LBM_BatchGetTile(LBMBatch *batch, int index, int *tileX, int *tileY);
 int LBM_BatchSetTile(LBMBatch *batch, int index, int tileX);
+
+/* Schedule of a step: LBM_BATCH_FUSED (one kernel launch per step for up to
+ * 64 grids of one collision operator) or LBM_BATCH_GRAPH (each grid's own
+ * step kernel, grids spread over 4 concurrent streams); both replayed from a
+ * CUDA graph of 32 steps.  LBM_BatchAutotune picks the faster one. */
+#define LBM_BATCH_FUSED 0
+#define LBM_BATCH_GRAPH 1
+int LBM_BatchGetSchedule(LBMBatch *batch);
+int LBM_BatchSetSchedule(LBMBatch *batch, int schedule);
 
 /* 256-cell tiles of one batched step over all grids, and the CUDA stream of
  * the batch. */

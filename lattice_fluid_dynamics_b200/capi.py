@@ -148,6 +148,8 @@ SIGNATURES = {
     "LBM_BatchGetTile": (C.c_int, [_vp, C.c_int, _vp, _vp]),
     "LBM_BatchSetTile": (C.c_int, [_vp, C.c_int, C.c_int]),
     "LBM_BatchTilesPerStep": (C.c_longlong, [_vp]),
+    "LBM_BatchGetSchedule": (C.c_int, [_vp]),
+    "LBM_BatchSetSchedule": (C.c_int, [_vp, C.c_int]),
     "LBM_BatchGetStream": (_vp, [_vp]),
     "LBM_NNKPad": (C.c_int, [C.c_int]),
     "LBM_NNConvForward": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, C.c_int,
@@ -604,6 +606,14 @@ class Batch:
     def set_tile(self, i: int, tile_x: int):
         if self._L.LBM_BatchSetTile(self._b, i, tile_x) != 0:
             raise ValueError(f"tile width {tile_x}")
+
+    @property
+    def schedule(self) -> str:
+        return ("fused", "graph")[self._L.LBM_BatchGetSchedule(self._b)]
+
+    def set_schedule(self, name: str):
+        if self._L.LBM_BatchSetSchedule(self._b, {"fused": 0, "graph": 1}[name]) != 0:
+            raise ValueError(name)
 
     @property
     def tiles_per_step(self) -> int:

@@ -1,14 +1,17 @@
-// Batched sweeps (LBM_Batch*): one kernel launch per lattice step advances
-// up to 64 grids of one operator (a batch takes one launch per operator and
-// per 64 grids).
+// Batched sweeps (LBM_Batch*): many independent grids advanced together.
 //
-// Each launch is k_step_batch over the concatenated tiles of its grids, the
-// per-grid arguments passed by value in the kernel parameter (two argument
-// sets, one per buffer parity, since consecutive steps swap source and
-// destination).  A CUDA graph of a 32-step chunk (A, B, A, B, ...) is
-// captured with those arguments and replayed while they stay the same.
-// Before a run the batch stream waits for every grid's stream; after it
-// every grid's stream waits for the batch.
+// Two schedules, chosen per batch by LBM_BatchAutotune from measurements:
+//   fused - one kernel launch per step for up to 64 grids of one collision
+//           operator (k_step_batch: the grids' tiles concatenated, each grid's
+//           arguments read from the kernel parameter);
+//   graph - every grid's own fused step kernel (k_step, the grid's tile
+//           shape), the grids spread over a few streams that run
+//           concurrently.
+// Either way a 32-step chunk is captured once as a CUDA graph and replayed
+// while the arguments stay the same (one graph launch per chunk), and every
+// grid's populations are bit-identical to stepping it alone.  Before a run
+// the batch stream waits for every grid's stream; after it every grid's
+// stream waits for the batch.
 //
 // Grids leaving an explicit-f state (after LBM_InitializeFlow or a
 // geometry edit) first take their priming steps through their own
@@ -25,28 +28,41 @@
 
 using namespace lbm;
 
+namespace {
+enum { MODE_FUSED = 0, MODE_GRAPH = 1 };
+constexpr int kChunk = 32;    // even: buffer parity repeats after a replay
+constexpr int kStreams = 4;   // concurrent streams of the graph schedule
+}  // namespace
+
 struct LBMBatch {
     int count = 0;
     int storage = LBM_STORAGE_FP32;
+    int mode = MODE_FUSED;
     std::vector<LBMGrid *> grids;
     std::vector<int> lbx;                 // tile width exponent per grid
     std::vector<cudaEvent_t> grid_done;   // recorded on each grid's stream
     cudaEvent_t batch_done = nullptr;
+    cudaEvent_t fork = nullptr;
     cudaStream_t stream = nullptr;
-    // launch groups: grid indices, ordered by operator, at most
-    // BATCH_LAUNCH_MAX per group; arguments of both buffer parities
+    cudaStream_t side[kStreams] = {};
+    cudaEvent_t side_done[kStreams] = {};
+    std::vector<int> lane;                // stream of each grid (graph schedule)
+    // fused schedule: launch groups (one operator, <= BATCH_LAUNCH_MAX grids)
     std::vector<std::vector<int>> groups;
     std::vector<BatchLaunchParams> params[2];
     std::vector<int> sets;
-    // the CUDA graph of kChunk steps and the arguments it was captured with
+    // graph schedule: each grid's step arguments of both buffer parities
+    std::vector<StepArgs> args[2];
+    // the captured chunk and what it was captured with
     cudaGraphExec_t graph = nullptr;
+    int graph_mode = -1;
     std::vector<BatchLaunchParams> graph_params[2];
     std::vector<int> graph_sets;
+    std::vector<StepArgs> graph_args[2];
+    std::vector<int> graph_lbx;
 };
 
 namespace {
-
-constexpr int kChunk = 32;  // even: buffer parity repeats after a replay
 
 GridImpl *impl(LBMGrid *g) { return static_cast<GridImpl *>(g->impl); }
 
@@ -59,12 +75,49 @@ int set_of(unsigned used) {
     return BATCH_SET_ALL;
 }
 
-BatchEntry make_entry(LBMGrid *g, int lbx, const void *src, void *dst, const float in[3]) {
+StepArgs step_of(LBMGrid *g, const void *src, void *dst, const float in[3]) {
+    StepArgs a = grid_step_args(g, in[0], in[1], in[2]);
+    a.src = src;
+    a.dst = dst;
+    a.periodic = impl(g)->stream_periodic;
+    return a;
+}
+
+bool same_args(const StepArgs &a, const StepArgs &b) {
+    return a.src == b.src && a.dst == b.dst && a.flags == b.flags && a.slot == b.slot &&
+           a.bmask == b.bmask && a.bfirst == b.bfirst && a.lq == b.lq && a.nx == b.nx &&
+           a.ny == b.ny && a.nz == b.nz && a.n == b.n && a.periodic == b.periodic &&
+           a.tau == b.tau && a.omega == b.omega && a.smag18 == b.smag18 &&
+           a.omega_d == b.omega_d && a.smag18_d == b.smag18_d && a.inX == b.inX &&
+           a.inY == b.inY && a.inZ == b.inZ && a.guard == b.guard;
+}
+
+bool same_params(const std::vector<BatchLaunchParams> &x, const std::vector<BatchLaunchParams> &y) {
+    if (x.size() != y.size()) return false;
+    for (size_t i = 0; i < x.size(); i++) {
+        const BatchLaunchParams &a = x[i], &b = y[i];
+        if (a.count != b.count) return false;
+        for (int j = 0; j <= a.count; j++)
+            if (a.starts[j] != b.starts[j]) return false;
+        for (int j = 0; j < a.count; j++)
+            if (!same_args(a.e[j].a, b.e[j].a) || a.e[j].combo != b.e[j].combo ||
+                a.e[j].lbx != b.e[j].lbx || a.e[j].tiles_x != b.e[j].tiles_x ||
+                a.e[j].tiles_y != b.e[j].tiles_y)
+                return false;
+    }
+    return true;
+}
+
+bool same_arg_vec(const std::vector<StepArgs> &x, const std::vector<StepArgs> &y) {
+    if (x.size() != y.size()) return false;
+    for (size_t i = 0; i < x.size(); i++)
+        if (!same_args(x[i], y[i])) return false;
+    return true;
+}
+
+BatchEntry make_entry(LBMGrid *g, int lbx, const StepArgs &a) {
     BatchEntry e{};
-    e.a = grid_step_args(g, in[0], in[1], in[2]);
-    e.a.src = src;
-    e.a.dst = dst;
-    e.a.periodic = impl(g)->stream_periodic;
+    e.a = a;
     e.combo = combo_of(g);
     e.lbx = lbx;
     const int bx = 1 << lbx, by = 256 >> lbx;
@@ -101,10 +154,80 @@ void make_groups(LBMBatch &b) {
     }
 }
 
-bool same_params(const std::vector<BatchLaunchParams> &a, const std::vector<BatchLaunchParams> &c) {
-    if (a.size() != c.size()) return false;
-    for (size_t i = 0; i < a.size(); i++)
-        if (memcmp(&a[i], &c[i], sizeof(BatchLaunchParams)) != 0) return false;
+// streams of the graph schedule: largest grids first onto the least loaded
+void make_lanes(LBMBatch &b) {
+    std::vector<int> order(b.count);
+    for (int i = 0; i < b.count; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return impl(b.grids[x])->n > impl(b.grids[y])->n; });
+    long long load[kStreams] = {0};
+    b.lane.assign(b.count, 0);
+    for (int i : order) {
+        int best = 0;
+        for (int s = 1; s < kStreams; s++)
+            if (load[s] < load[best]) best = s;
+        b.lane[i] = best;
+        load[best] += impl(b.grids[i])->n;
+    }
+}
+
+// fused launch arguments of every group for per-grid step arguments a[i]
+bool build_params(LBMBatch &b, const std::vector<StepArgs> &a, std::vector<BatchLaunchParams> &out,
+                  std::vector<int> &sets) {
+    out.assign(b.groups.size(), BatchLaunchParams{});
+    sets.assign(b.groups.size(), BATCH_SET_ALL);
+    for (size_t gi = 0; gi < b.groups.size(); gi++) {
+        const std::vector<int> &grp = b.groups[gi];
+        unsigned used = 0;
+        long long total = 0;
+        for (size_t j = 0; j < grp.size(); j++) {
+            const int i = grp[j];
+            out[gi].e[j] = make_entry(b.grids[i], b.lbx[i], a[i]);
+            out[gi].starts[j] = (unsigned)total;
+            total += units_of(out[gi].e[j], impl(b.grids[i])->nz);
+            used |= 1u << combo_of(b.grids[i]);
+        }
+        if (total > 0x7fffffffLL) return false;
+        out[gi].starts[grp.size()] = (unsigned)total;
+        out[gi].count = (int)grp.size();
+        sets[gi] = set_of(used);
+    }
+    return true;
+}
+
+// the grid's fused step kernel with the batch's tile shape for it
+cudaError_t grid_step(LBMBatch &b, int i, const StepArgs &a, cudaStream_t s) {
+    GridImpl t = *impl(b.grids[i]);
+    t.bx = 1 << b.lbx[i];
+    t.by = 256 >> b.lbx[i];
+    t.cpt = 1;
+    t.minb = 4;
+    const int op = grid_op(b.grids[i]);
+    return launch_step(t, a, true, op, b.grids[i]->useSmagorinsky == 1, false, s);
+}
+
+// `steps` steps of the whole batch in the graph schedule: forked from the
+// batch stream onto the side streams, each stream stepping its grids with
+// the arguments of alternating parity (a[0], a[1], a[0], ...), joined back
+// at the end; grids on different streams run concurrently
+bool steps_graph(LBMBatch &b, const std::vector<StepArgs> *a, int steps) {
+    LBMGrid *g0 = b.grids[0];
+    if (fail(g0, cudaEventRecord(b.fork, b.stream))) return false;
+    for (int s = 0; s < kStreams; s++)
+        if (fail(g0, cudaStreamWaitEvent(b.side[s], b.fork, 0))) return false;
+    for (int k = 0; k < steps; k++)
+        for (int i = 0; i < b.count; i++)
+            if (fail(b.grids[i], grid_step(b, i, a[k & 1][i], b.side[b.lane[i]]))) return false;
+    for (int s = 0; s < kStreams; s++)
+        if (fail(g0, cudaEventRecord(b.side_done[s], b.side[s])) ||
+            fail(g0, cudaStreamWaitEvent(b.stream, b.side_done[s], 0)))
+            return false;
+    return true;
+}
+
+bool step_fused(LBMBatch &b, const std::vector<BatchLaunchParams> &p, const std::vector<int> &sets) {
+    for (size_t gi = 0; gi < p.size(); gi++)
+        if (fail(b.grids[0], launch_step_batch(b.storage, p[gi], sets[gi], b.stream))) return false;
     return true;
 }
 
@@ -133,12 +256,20 @@ LBMBatch *LBM_BatchCreate(LBMGrid **grids, int count) {
     b->grid_done.assign(count, nullptr);
     bool good = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess;
     good = good && cudaEventCreateWithFlags(&b->batch_done, cudaEventDisableTiming) == cudaSuccess;
+    good = good && cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int s = 0; good && s < kStreams; s++) {
+        good = cudaStreamCreateWithFlags(&b->side[s], cudaStreamNonBlocking) == cudaSuccess;
+        good = good &&
+               cudaEventCreateWithFlags(&b->side_done[s], cudaEventDisableTiming) == cudaSuccess;
+    }
     for (int i = 0; good && i < count; i++)
         good = cudaEventCreateWithFlags(&b->grid_done[i], cudaEventDisableTiming) == cudaSuccess;
     if (!good) {
         LBM_BatchFree(b);
         return nullptr;
     }
+    make_groups(*b);
+    make_lanes(*b);
     return b;
 }
 
@@ -149,6 +280,11 @@ void LBM_BatchFree(LBMBatch *b) {
     for (cudaEvent_t e : b->grid_done)
         if (e) cudaEventDestroy(e);
     if (b->batch_done) cudaEventDestroy(b->batch_done);
+    if (b->fork) cudaEventDestroy(b->fork);
+    for (int s = 0; s < kStreams; s++) {
+        if (b->side[s]) cudaStreamDestroy(b->side[s]);
+        if (b->side_done[s]) cudaEventDestroy(b->side_done[s]);
+    }
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -178,34 +314,19 @@ int LBM_BatchRun(LBMBatch *b, int nSteps, const float *inlet) {
     const int steps = nSteps - prime;
     if (steps == 0) return LBM_OK;
 
-    // launch arguments of both parities for every group
-    make_groups(*b);
-    const size_t ng = b->groups.size();
-    for (int p = 0; p < 2; p++) b->params[p].assign(ng, BatchLaunchParams{});
-    b->sets.assign(ng, BATCH_SET_ALL);
-    for (size_t gi = 0; gi < ng; gi++) {
-        const std::vector<int> &grp = b->groups[gi];
-        unsigned used = 0;
-        long long total = 0;
-        for (size_t j = 0; j < grp.size(); j++) {
-            const int i = grp[j];
-            LBMGrid *g = b->grids[i];
-            GridImpl &I = *impl(g);
-            if (I.fbuf >= 0 || I.stream_periodic != g->periodicYZ) return LBM_ERR_CUDA;
-            const float *in = inlet + 3 * i;
-            b->params[0][gi].e[j] = make_entry(g, b->lbx[i], I.pop[I.gbuf], I.pop[1 - I.gbuf], in);
-            b->params[1][gi].e[j] = make_entry(g, b->lbx[i], I.pop[1 - I.gbuf], I.pop[I.gbuf], in);
-            b->params[0][gi].starts[j] = b->params[1][gi].starts[j] = (unsigned)total;
-            total += units_of(b->params[0][gi].e[j], I.nz);
-            used |= 1u << combo_of(g);
-        }
-        if (total > 0x7fffffffLL) return LBM_ERR_INVALID_ARGUMENT;
-        for (int p = 0; p < 2; p++) {
-            b->params[p][gi].starts[grp.size()] = (unsigned)total;
-            b->params[p][gi].count = (int)grp.size();
-        }
-        b->sets[gi] = set_of(used);
+    // step arguments of both buffer parities
+    make_groups(*b);  // operators may have changed between runs
+    for (int p = 0; p < 2; p++) b->args[p].resize(n);
+    for (int i = 0; i < n; i++) {
+        LBMGrid *g = b->grids[i];
+        GridImpl &I = *impl(g);
+        if (I.fbuf >= 0 || I.stream_periodic != g->periodicYZ) return LBM_ERR_CUDA;
+        b->args[0][i] = step_of(g, I.pop[I.gbuf], I.pop[1 - I.gbuf], inlet + 3 * i);
+        b->args[1][i] = step_of(g, I.pop[1 - I.gbuf], I.pop[I.gbuf], inlet + 3 * i);
     }
+    if (b->mode == MODE_FUSED && (!build_params(*b, b->args[0], b->params[0], b->sets) ||
+                                  !build_params(*b, b->args[1], b->params[1], b->sets)))
+        return LBM_ERR_INVALID_ARGUMENT;
 
     // the batch waits for every grid's queued work
     for (int i = 0; i < n; i++) {
@@ -214,22 +335,28 @@ int LBM_BatchRun(LBMBatch *b, int nSteps, const float *inlet) {
         if (fail(b->grids[i], cudaStreamWaitEvent(b->stream, b->grid_done[i], 0)))
             return LBM_ERR_CUDA;
     }
-    auto step = [&](int parity) {
-        for (size_t gi = 0; gi < ng; gi++)
-            if (fail(g0, launch_step_batch(b->storage, b->params[parity][gi], b->sets[gi],
-                                           b->stream)))
-                return false;
+    // `k` steps from parity 0 (k even keeps the parity)
+    auto run = [&](int k) {
+        if (b->mode == MODE_GRAPH) return k == 0 || steps_graph(*b, b->args, k);
+        for (int j = 0; j < k; j++)
+            if (!step_fused(*b, b->params[j & 1], b->sets)) return false;
         return true;
     };
     int left = steps;
     if (left >= kChunk) {
-        if (!b->graph || b->graph_sets != b->sets || !same_params(b->graph_params[0], b->params[0]) ||
-            !same_params(b->graph_params[1], b->params[1])) {
+        bool stale = !b->graph || b->graph_mode != b->mode;
+        if (!stale && b->mode == MODE_FUSED)
+            stale = b->graph_sets != b->sets || !same_params(b->graph_params[0], b->params[0]) ||
+                    !same_params(b->graph_params[1], b->params[1]);
+        if (!stale && b->mode == MODE_GRAPH)
+            stale = b->graph_lbx != b->lbx || !same_arg_vec(b->graph_args[0], b->args[0]) ||
+                    !same_arg_vec(b->graph_args[1], b->args[1]);
+        if (stale) {
             drop_graph(*b);
             cudaGraph_t graph = nullptr;
             bool good = !fail(g0, cudaStreamBeginCapture(b->stream,
                                                          cudaStreamCaptureModeThreadLocal));
-            for (int k = 0; good && k < kChunk; k++) good = step(k & 1);
+            good = good && run(kChunk);
             const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
             good = good && !fail(g0, e);
             cudaGraphExec_t exec = nullptr;
@@ -237,17 +364,20 @@ int LBM_BatchRun(LBMBatch *b, int nSteps, const float *inlet) {
             if (graph) cudaGraphDestroy(graph);
             if (!good) return LBM_ERR_CUDA;
             b->graph = exec;
+            b->graph_mode = b->mode;
             b->graph_params[0] = b->params[0];
             b->graph_params[1] = b->params[1];
             b->graph_sets = b->sets;
+            b->graph_args[0] = b->args[0];
+            b->graph_args[1] = b->args[1];
+            b->graph_lbx = b->lbx;
         }
         while (left >= kChunk) {
             if (fail(g0, cudaGraphLaunch(b->graph, b->stream))) return LBM_ERR_CUDA;
             left -= kChunk;
         }
     }
-    for (int k = 0; k < left; k++)
-        if (!step(k & 1)) return LBM_ERR_CUDA;
+    if (!run(left)) return LBM_ERR_CUDA;
 
     // every grid's later work waits for the batch
     if (fail(g0, cudaEventRecord(b->batch_done, b->stream))) return LBM_ERR_CUDA;
@@ -262,57 +392,80 @@ int LBM_BatchRun(LBMBatch *b, int nSteps, const float *inlet) {
 int LBM_BatchAutotune(LBMBatch *b, int trialLaunches) {
     if (!b || trialLaunches <= 0) return LBM_ERR_INVALID_ARGUMENT;
     LBMGrid *g0 = b->grids[0];
-    // scratch destination large enough for the largest grid, and a guard
-    // counter nobody reads
-    long long nmax = 0;
-    for (LBMGrid *g : b->grids) nmax = impl(g)->n > nmax ? impl(g)->n : nmax;
-    void *scratch = nullptr;
+    const int n = b->count;
+    // Time the launch each grid's next step would make, in place: once its
+    // velocity is materialised, the buffer that step writes holds nothing
+    // the grid still needs, and the next step overwrites it anyway.
     unsigned long long *guard = nullptr;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
-    bool good = !fail(g0, cudaMalloc(&scratch, (size_t)nmax * 19 * impl(g0)->elem)) &&
-                !fail(g0, cudaMalloc(&guard, sizeof(unsigned long long))) &&
+    bool good = !fail(g0, cudaMalloc(&guard, sizeof(unsigned long long))) &&
                 !fail(g0, cudaEventCreate(&t0)) && !fail(g0, cudaEventCreate(&t1));
-    for (int i = 0; i < b->count; i++)
-        good = good && !fail(b->grids[i], cudaStreamSynchronize(impl(b->grids[i])->stream));
-    good = good && !fail(g0, cudaStreamSynchronize(b->stream));
-    BatchLaunchParams p{};
-    for (int i = 0; good && i < b->count; i++) {
+    std::vector<StepArgs> a(n);
+    for (int i = 0; good && i < n; i++) {
         LBMGrid *g = b->grids[i];
         GridImpl &I = *impl(g);
-        const void *src = I.fbuf >= 0 ? I.pop[I.fbuf] : I.pop[I.gbuf];
+        good = grid_ensure_velocity(g) && !fail(g, cudaStreamSynchronize(I.stream));
         const float in[3] = {I.vin_inlet[0], I.vin_inlet[1], I.vin_inlet[2]};
-        float best = 1e30f;
-        int best_lbx = b->lbx[i];
-        for (int lbx = 5; good && lbx <= 8; lbx++) {
-            p.e[0] = make_entry(g, lbx, src, scratch, in);
-            p.e[0].a.guard = guard;
+        a[i] = I.fbuf >= 0 ? step_of(g, I.pop[I.fbuf], I.pop[I.gbuf], in)
+                           : step_of(g, I.pop[I.gbuf], I.pop[1 - I.gbuf], in);
+        a[i].guard = guard;
+    }
+    good = good && !fail(g0, cudaStreamSynchronize(b->stream));
+    auto timed = [&](auto &&launch) -> float {
+        if (!good) return 0.f;
+        good = launch();  // one untimed launch first
+        good = good && !fail(g0, cudaEventRecord(t0, b->stream));
+        for (int k = 0; good && k < trialLaunches; k++) good = launch();
+        good = good && !fail(g0, cudaEventRecord(t1, b->stream)) &&
+               !fail(g0, cudaEventSynchronize(t1));
+        float ms = 0;
+        good = good && !fail(g0, cudaEventElapsedTime(&ms, t0, t1));
+        return ms;
+    };
+    // per grid and schedule, the fastest tile shape (a wider tile must be at
+    // least 2 % faster to replace a narrower one)
+    std::vector<int> lbx_fused(n, 5), lbx_graph(n, 5);
+    for (int i = 0; good && i < n; i++) {
+        float best_f = 1e30f, best_g = 1e30f;
+        for (int l = 5; good && l <= 8; l++) {
+            BatchLaunchParams p{};
+            p.e[0] = make_entry(b->grids[i], l, a[i]);
             p.starts[0] = 0;
-            p.starts[1] = (unsigned)units_of(p.e[0], I.nz);
+            p.starts[1] = (unsigned)units_of(p.e[0], impl(b->grids[i])->nz);
             p.count = 1;
             const int set = set_of(1u << p.e[0].combo);
-            // one untimed launch, then the timed ones
-            good = !fail(g, launch_step_batch(b->storage, p, set, b->stream)) &&
-                   !fail(g, cudaEventRecord(t0, b->stream));
-            for (int k = 0; good && k < trialLaunches; k++)
-                good = !fail(g, launch_step_batch(b->storage, p, set, b->stream));
-            good = good && !fail(g, cudaEventRecord(t1, b->stream)) &&
-                   !fail(g, cudaEventSynchronize(t1));
-            float ms = 0;
-            good = good && !fail(g, cudaEventElapsedTime(&ms, t0, t1));
-            // a wider tile must be at least 2 % faster to replace a narrower one
-            if (good && ms < best * 0.98f) {
-                best = ms;
-                best_lbx = lbx;
-            }
-        }
-        if (good && best_lbx != b->lbx[i]) {
-            b->lbx[i] = best_lbx;
-            drop_graph(*b);
+            const float mf = timed([&] {
+                return !fail(g0, launch_step_batch(b->storage, p, set, b->stream));
+            });
+            if (good && mf < best_f * 0.98f) best_f = mf, lbx_fused[i] = l;
+            b->lbx[i] = l;
+            const float mg = timed([&] { return !fail(g0, grid_step(*b, i, a[i], b->stream)); });
+            if (good && mg < best_g * 0.98f) best_g = mg, lbx_graph[i] = l;
         }
     }
+    // the whole batch, one step, in each schedule with its tiles
+    float ms_fused = 1e30f, ms_graph = 1e30f;
+    if (good) {
+        b->lbx = lbx_fused;
+        make_groups(*b);
+        std::vector<BatchLaunchParams> p;
+        std::vector<int> sets;
+        good = build_params(*b, a, p, sets);
+        ms_fused = timed([&] { return step_fused(*b, p, sets); });
+    }
+    if (good) {
+        b->lbx = lbx_graph;
+        const std::vector<StepArgs> both[2] = {a, a};
+        ms_graph = timed([&] { return steps_graph(*b, both, 1); });
+    }
+    if (good) {
+        b->mode = ms_graph < ms_fused ? MODE_GRAPH : MODE_FUSED;
+        b->lbx = b->mode == MODE_GRAPH ? lbx_graph : lbx_fused;
+        drop_graph(*b);
+    }
+    good = good && !fail(g0, cudaStreamSynchronize(b->stream));
     if (t0) cudaEventDestroy(t0);
     if (t1) cudaEventDestroy(t1);
-    cudaFree(scratch);
     cudaFree(guard);
     return good ? LBM_OK : LBM_ERR_CUDA;
 }
@@ -332,6 +485,15 @@ int LBM_BatchSetTile(LBMBatch *b, int index, int tileX) {
     if (lbx < 0) return LBM_ERR_INVALID_ARGUMENT;
     if (b->lbx[index] != lbx) drop_graph(*b);
     b->lbx[index] = lbx;
+    return LBM_OK;
+}
+
+int LBM_BatchGetSchedule(LBMBatch *b) { return b ? b->mode : -1; }
+
+int LBM_BatchSetSchedule(LBMBatch *b, int schedule) {
+    if (!b || (schedule != MODE_FUSED && schedule != MODE_GRAPH)) return LBM_ERR_INVALID_ARGUMENT;
+    if (b->mode != schedule) drop_graph(*b);
+    b->mode = schedule;
     return LBM_OK;
 }
 

@@ -232,6 +232,7 @@ bool grid_enqueue_step(LBMGrid *grid, float inX, float inY, float inZ) {
     return enqueue_step(grid, inX, inY, inZ);
 }
 bool grid_ok(LBMGrid *grid, cudaError_t e) { return ok(grid, e); }
+bool grid_ensure_velocity(LBMGrid *grid) { return ensure_vel(grid); }
 void grid_note_fused_steps(LBMGrid *grid, int k, float inX, float inY, float inZ) {
     GridImpl &I = *IMPL(grid);
     if (k <= 0) return;

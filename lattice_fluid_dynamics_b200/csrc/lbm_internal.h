@@ -125,6 +125,9 @@ bool grid_enqueue_step(LBMGrid *grid, float inX, float inY, float inZ);
 // the state transition of k fused steps run outside the grid's own launcher
 void grid_note_fused_steps(LBMGrid *grid, int k, float inX, float inY, float inZ);
 bool grid_ok(LBMGrid *grid, cudaError_t e);
+// materialise the velocity of the last step (after which the buffer that step
+// read is free until the next step)
+bool grid_ensure_velocity(LBMGrid *grid);
 // f = f_new = feq(rho, u) from device fields rho[n], u[3n]; returns 1 or 0
 int grid_init_from_device(LBMGrid *grid, const float *drho, const float *du);
 

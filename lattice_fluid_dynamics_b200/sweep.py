@@ -81,7 +81,7 @@ def run_sweep(count: int = 64, steps: int = 3000, seed: int = 1, autotune: bool 
         "cells_total": int(cells.sum()), "ms": ms,
         "mlups": total / (ms * 1e-3) / 1e6,
         "gb_per_s": total * grids[0].bytes_per_update() / (ms * 1e-3) / 1e9,
-        "tiles_per_step": batch.tiles_per_step,
+        "tiles_per_step": batch.tiles_per_step, "schedule": batch.schedule,
         "setup_s": setup_s, "autotune_s": tune_s,
         "per_instance": [],
     }

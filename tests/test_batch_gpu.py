@@ -33,11 +33,13 @@ def _inlets(mix):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("schedule", ["fused", "graph"])
 @pytest.mark.parametrize("runs", [[70], [1, 1, 33], [3, 64, 5]])
-def test_batch_matches_solo(solver, runs):
+def test_batch_matches_solo(solver, runs, schedule):
     bg = [_make(solver, m) for m in MIX]
     sg = [_make(solver, m) for m in MIX]
     b = capi.Batch(bg)
+    b.set_schedule(schedule)
     for n in runs:
         b.run(n, _inlets(MIX))
         for g, m in zip(sg, MIX):
@@ -63,11 +65,13 @@ def test_batch_matches_oracle(solver, oracle):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("schedule", ["fused", "graph"])
 @pytest.mark.parametrize("tile", [32, 64, 128, 256])
-def test_tiles_do_not_change_results(solver, tile):
+def test_tiles_do_not_change_results(solver, tile, schedule):
     bg = [_make(solver, m) for m in MIX]
     sg = [_make(solver, m) for m in MIX]
     b = capi.Batch(bg)
+    b.set_schedule(schedule)
     for i in range(len(bg)):
         b.set_tile(i, tile)
         assert b.tile(i) == (tile, 256 // tile)
@@ -86,6 +90,7 @@ def test_autotune_leaves_state_and_interleaves_with_solo_calls(solver):
     b.run(5, _inlets(MIX))
     before = [g.populations() for g in bg]
     b.autotune(3)
+    assert b.schedule in ("fused", "graph")
     for g, f in zip(bg, before):
         assert np.array_equal(g.populations(), f)
     assert all(b.tile(i)[0] in (32, 64, 128, 256) for i in range(len(bg)))
