@@ -254,6 +254,14 @@ const char *LBM_GetErrorString(int code);
  * stores of the storage type): 152 FP32, 76 FP16/BF16, 304 FP64. */
 int LBM_BytesPerUpdate(LBMGrid *grid);
 
+/* Fused steps of 32 x 8 launch tiles can stage their pull neighbourhood in
+ * shared memory with TMA bulk tensor copies (FP32 / FP16 / BF16 storage,
+ * sizeX * element size a multiple of 16 bytes); results are identical to
+ * the direct kernel's.  enable = 0 turns it off, 1 on where possible; the
+ * return value is whether it is on.  On by default unless LBM_TMA=0 is set
+ * in the environment when the grid is created. */
+int LBM_SetTMAStaging(LBMGrid *grid, int enable);
+
 /* ---------------------------------------------------------------------
  * Particles (particle_lbm.comp:46-89 trilinear sampler, :207-293 Euler
  * step with collisionMode 0).  Particles live in device memory.

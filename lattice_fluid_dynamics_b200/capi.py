@@ -127,6 +127,7 @@ SIGNATURES = {
     "LBM_GetLastError": (C.c_int, [_G]),
     "LBM_GetErrorString": (C.c_char_p, [C.c_int]),
     "LBM_BytesPerUpdate": (C.c_int, [_G]),
+    "LBM_SetTMAStaging": (C.c_int, [_G, C.c_int]),
     "LBM_ParticlesCreate": (_vp, [C.c_int, C.c_uint]),
     "LBM_ParticlesFree": (None, [_vp]),
     "LBM_ParticlesStep": (C.c_int, [_vp, _G, _f]),
@@ -398,6 +399,10 @@ class Grid:
 
     def bytes_per_update(self) -> int:
         return int(self._L.LBM_BytesPerUpdate(self._g))
+
+    def set_tma_staging(self, enable: bool) -> bool:
+        """Turn the TMA-staged step kernel on or off; returns whether it is on."""
+        return bool(self._L.LBM_SetTMAStaging(self._g, 1 if enable else 0))
 
 
 class Particles:

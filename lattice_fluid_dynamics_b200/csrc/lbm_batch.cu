@@ -89,7 +89,7 @@ bool same_args(const StepArgs &a, const StepArgs &b) {
            a.ny == b.ny && a.nz == b.nz && a.n == b.n && a.periodic == b.periodic &&
            a.tau == b.tau && a.omega == b.omega && a.smag18 == b.smag18 &&
            a.omega_d == b.omega_d && a.smag18_d == b.smag18_d && a.inX == b.inX &&
-           a.inY == b.inY && a.inZ == b.inZ && a.guard == b.guard;
+           a.inY == b.inY && a.inZ == b.inZ && a.guard == b.guard && a.err == b.err;
 }
 
 bool same_params(const std::vector<BatchLaunchParams> &x, const std::vector<BatchLaunchParams> &y) {

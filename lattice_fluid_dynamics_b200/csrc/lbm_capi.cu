@@ -146,6 +146,7 @@ StepArgs step_args(LBMGrid *grid, GridImpl &I, float inX, float inY, float inZ) 
     a.inY = inY;
     a.inZ = inZ;
     a.guard = I.guard;
+    a.err = I.err_flag;
     return a;
 }
 
@@ -338,6 +339,7 @@ LBMGrid *LBM_CreateEx(int sizeX, int sizeY, int sizeZ, float viscosity, int stor
         LBM_Free(grid);
         return nullptr;
     }
+    setup_tma(*I, false);
     I->fbuf = 0;
     I->gbuf = 1;
     I->vel_valid = true;
@@ -790,6 +792,18 @@ void *LBM_GetStream(LBMGrid *grid) {
 int LBM_BytesPerUpdate(LBMGrid *grid) {
     GridImpl *I = IMPL(grid);
     return I ? (int)(38 * I->elem) : 0;
+}
+
+int LBM_SetTMAStaging(LBMGrid *grid, int enable) {
+    GridImpl *I = IMPL(grid);
+    if (!I) return 0;
+    if (!enable) {
+        I->tma = false;
+    } else if (!I->tma) {
+        setup_tma(*I, true);
+    }
+    drop_graph(*I);  // captured steps name the kernel
+    return I->tma ? 1 : 0;
 }
 
 // vti_export.c:10-116

@@ -70,11 +70,13 @@ enum : uint8_t {
 // FP16/BF16 keep the deviation f_i - w_i (w_i in FP32).
 // ---------------------------------------------------------------------
 // load2/store2 move the populations of two neighbouring cells (p must be
-// aligned to two elements).
+// aligned to two elements).  `load` reads global memory through the
+// read-only path; `lds` reads a population staged in shared memory.
 struct StoreF32 {
     using T = float;
     using R = float;
     static __device__ __forceinline__ R load(const T *p, int) { return __ldg(p); }
+    static __device__ __forceinline__ R lds(const T *p, int) { return *p; }
     static __device__ __forceinline__ void store(T *p, R v, int) { *p = v; }
     static __device__ __forceinline__ void load2(const T *p, int, R &a, R &b) {
         const float2 v = __ldg(reinterpret_cast<const float2 *>(p));
@@ -89,6 +91,7 @@ struct StoreF64 {
     using T = double;
     using R = double;
     static __device__ __forceinline__ R load(const T *p, int) { return __ldg(p); }
+    static __device__ __forceinline__ R lds(const T *p, int) { return *p; }
     static __device__ __forceinline__ void store(T *p, R v, int) { *p = v; }
     static __device__ __forceinline__ void load2(const T *p, int, R &a, R &b) {
         const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
@@ -104,6 +107,9 @@ struct StoreF16 {
     using R = float;
     static __device__ __forceinline__ R load(const T *p, int i) {
         return __half2float(__ldg(p)) + wgt<float>(i);
+    }
+    static __device__ __forceinline__ R lds(const T *p, int i) {
+        return __half2float(*p) + wgt<float>(i);
     }
     static __device__ __forceinline__ void store(T *p, R v, int i) {
         *p = __float2half_rn(v - wgt<float>(i));
@@ -123,6 +129,9 @@ struct StoreBF16 {
     using R = float;
     static __device__ __forceinline__ R load(const T *p, int i) {
         return __bfloat162float(__ldg(p)) + wgt<float>(i);
+    }
+    static __device__ __forceinline__ R lds(const T *p, int i) {
+        return __bfloat162float(*p) + wgt<float>(i);
     }
     static __device__ __forceinline__ void store(T *p, R v, int i) {
         *p = __float2bfloat16_rn(v - wgt<float>(i));

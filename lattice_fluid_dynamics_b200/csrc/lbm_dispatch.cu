@@ -1,5 +1,8 @@
 // Storage-format dispatch of the step kernels (instantiated in
 // lbm_step_{f32,f64,f16,bf16}.cu).
+#include <cudaTypedefs.h>
+#include <stdlib.h>
+
 #include "lbm_step.cuh"
 
 namespace lbm {
@@ -9,6 +12,14 @@ extern template struct exact::StepLaunch<exact::StoreF32>;
 extern template struct exact::StepLaunch<exact::StoreF64>;
 extern template struct exact::StepLaunch<exact::StoreF16>;
 extern template struct exact::StepLaunch<exact::StoreBF16>;
+
+#define LBM_DISPATCH_INTO(out, storage, CALL)                        \
+    switch (storage) {                                                \
+        case LBM_STORAGE_FP32: out = StepLaunch<StoreF32>::CALL; break; \
+        case LBM_STORAGE_FP16: out = StepLaunch<StoreF16>::CALL; break; \
+        case LBM_STORAGE_BF16: out = StepLaunch<StoreBF16>::CALL; break; \
+        default: out = cudaErrorNotSupported; break;                  \
+    }
 
 #define LBM_DISPATCH(storage, CALL)                               \
     switch (storage) {                                            \
@@ -28,6 +39,61 @@ cudaError_t launch_step(const GridImpl &g, const StepArgs &a, bool fused, int op
 
 cudaError_t launch_step_batch(int storage, const BatchLaunchParams &p, int set, cudaStream_t s) {
     LBM_DISPATCH(storage, batch(p, set, s));
+}
+
+// the driver's tensor-map encoder, looked up once through the runtime
+static PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+        }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// Each population buffer as a rank-4 tensor (x, y, z, direction) with boxes
+// of tma_box_x x TMA_BOX_Y x 1 x 1 elements, zero fill outside the grid.
+void setup_tma(GridImpl &g, bool force) {
+    g.tma = false;
+    const char *env = getenv("LBM_TMA");
+    if (!force && env && atoi(env) == 0) return;
+    CUtensorMapDataType dt;
+    switch (g.storage) {
+        case LBM_STORAGE_FP32: dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT32; break;
+        case LBM_STORAGE_FP16: dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT16; break;
+        case LBM_STORAGE_BF16: dt = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16; break;
+        default: return;
+    }
+    const size_t es = g.elem;
+    if (((size_t)g.nx * es) % 16 != 0 || !g.pop[0] || !g.pop[1]) return;
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = tma_encoder();
+    if (!enc) return;
+    const cuuint64_t dims[4] = {(cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)g.nz, 19};
+    const cuuint64_t strides[3] = {(cuuint64_t)g.nx * es, (cuuint64_t)g.nx * g.ny * es,
+                                   (cuuint64_t)g.n * es};
+    const cuuint32_t box[4] = {(cuuint32_t)tma_box_x(es), (cuuint32_t)TMA_BOX_Y, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    for (int k = 0; k < 2; k++) {
+        if (enc(&g.tmap[k], dt, 4, g.pop[k], dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return;
+    }
+    cudaError_t e = cudaSuccess;
+    LBM_DISPATCH_INTO(e, g.storage, tma_prepare());
+    if (e == cudaSuccess) e = fast::tma_prepare_fast(g.storage);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    g.tma = true;
 }
 
 static StepArgs stream_args(const GridImpl &g, const void *src, void *dst, int periodic) {

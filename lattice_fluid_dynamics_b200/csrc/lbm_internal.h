@@ -2,6 +2,7 @@
 // translation units of the library.  Not part of the public ABI.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -78,7 +79,28 @@ struct GridImpl {
     // CUDA graphs for LBM_StepN, one per starting buffer parity (gbuf)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int graph_key[2][8] = {{0}, {0}};
+
+    // TMA descriptors of the two population buffers as rank-4 tensors
+    // (x, y, z, direction); `tma` is set when they could be made (FP32 /
+    // FP16 / BF16 storage, rows a multiple of 16 bytes)
+    alignas(64) CUtensorMap tmap[2];
+    bool tma = false;
 };
+
+// The fused step with the pull neighbourhood staged in shared memory by TMA
+// (k_step_tma): tiles of 32 x TMA_BOX_Y cells, TMA_ZSEG z-planes per block.
+// The box of one direction spans the tile's 32 x plus tma_xpad() elements on
+// either side, so that its first x is a 16-byte multiple.
+constexpr int TMA_BOX_Y = 8, TMA_ZSEG = 8;
+__host__ __device__ constexpr int tma_xpad(size_t elem) { return (int)(16 / elem); }
+__host__ __device__ constexpr int tma_box_x(size_t elem) { return 32 + 2 * tma_xpad(elem); }
+__host__ __device__ constexpr int tma_stage_bytes(size_t elem) {
+    return 19 * tma_box_x(elem) * TMA_BOX_Y * (int)elem;
+}
+// dynamic shared memory of one block: barriers, alignment slack, 2 stages
+__host__ __device__ constexpr int tma_smem_bytes(size_t elem) {
+    return 256 + 2 * tma_stage_bytes(elem);
+}
 
 struct StepArgs {
     const void *src;   // populations read (post-collision g or explicit f)
@@ -95,6 +117,7 @@ struct StepArgs {
     double omega_d, smag18_d;   // the same in FP64 arithmetic (FP64 storage)
     float inX, inY, inZ;
     unsigned long long *guard;
+    int *err;          // device error word (bit 0: a TMA wait gave up)
 };
 
 // One grid of a batched step launch (k_step_batch): its step arguments,
@@ -149,7 +172,12 @@ cudaError_t launch_step(const GridImpl &g, const StepArgs &a, bool fused, int op
 namespace fast {
 cudaError_t launch_step_fast(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
                              cudaStream_t s);
+cudaError_t tma_prepare_fast(int storage);
 }
+// Encode the grid's TMA descriptors and allow k_step_tma's shared memory;
+// sets g.tma (false for FP64 storage or rows that are not a multiple of 16
+// bytes, or, unless `force`, when LBM_TMA=0 is set in the environment).
+void setup_tma(GridImpl &g, bool force);
 cudaError_t launch_stream_only(const GridImpl &g, const void *src, void *dst, int periodic,
                                cudaStream_t s);
 cudaError_t launch_velocity(const GridImpl &g, const void *src, int kind, int periodic,

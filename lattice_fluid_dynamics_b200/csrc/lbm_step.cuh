@@ -18,6 +18,7 @@
 
 #include "lbm_d3q19.cuh"
 #include "lbm_internal.h"
+#include "tc05.cuh"
 
 namespace lbm {
 namespace LBM_ARITH_NS {
@@ -254,6 +255,142 @@ __global__ void __launch_bounds__(256, MINB) k_step(const StepArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// The fused step with the pull neighbourhood staged in shared memory by TMA.
+//
+// A 32 x 8 thread block owns a 32 x TMA_BOX_Y tile of rows and walks up to
+// TMA_ZSEG z-planes.  For a plane z its 19 boxes are loaded by one thread:
+// direction i's box starts at (x0 - XPAD, y0 - e_y, z - e_z, i), so the
+// thread for cell (x0 + tx, y0 + ty) finds its pulled value f_i at row ty,
+// column tx + XPAD - e_x of that box.  Two stages alternate; each has an
+// mbarrier that completes when its 19 boxes have landed.  This trades the
+// 19 dependent read-only loads per cell for bulk copies that keep more bytes
+// in flight per SM, which is what limits the two-byte storage formats.
+//
+// Cells whose pull leaves the tile's interior rule (x, y or z on the grid
+// edge) pull directly from global memory with the wrap / clamp / own-value
+// rules of gather_pull; only interior cells read the staged boxes, so the
+// zero fill of boxes that overhang the grid is never read.  Bouzidi links,
+// collision, store and guard are those of step_cells: results are identical
+// to k_step's.  A wait that gives up (it never should) sets bit 0 of the
+// error word and the block finishes the remaining planes on the direct path
+// after a bounded wait for its copies in flight.
+constexpr uint32_t TMA_WAIT_LIMIT = 1u << 22;
+
+template <class S, int OP, bool SMAG>
+__device__ __forceinline__ int tma_cell(const StepArgs &a, const typename S::T *__restrict__ box,
+                                        bool staged, int x, int y, int z, int col) {
+    using T = typename S::T;
+    using R = typename S::R;
+    constexpr int BX = tma_box_x(sizeof(T));
+    constexpr int BOX = BX * TMA_BOX_Y;
+    const long long n = a.n;
+    const long long cell = (long long)x + (long long)a.nx * ((long long)y + (long long)a.ny * z);
+    const T *__restrict__ src = static_cast<const T *>(a.src);
+    T *__restrict__ dst = static_cast<T *>(a.dst);
+    const uint8_t flag = a.flags[cell];
+    R f[19], fn[19];
+    if (staged) {
+#pragma unroll
+        for (int i = 0; i < 19; i++) f[i] = S::lds(box + i * BOX + col - cx(i), i);
+    } else {
+        gather_pull<S>(a, src, x, neighbour_rows(a, y, z), cell, f);
+    }
+    if (flag & FLAG_BOUNDARY) bouzidi<S>(a, src, x, neighbour_rows(a, y, z), cell, f);
+    const int kind = collide_cell<S, OP, SMAG>(a, f, fn, x, flag);
+#pragma unroll
+    for (int i = 0; i < 19; i++) S::store(dst + (long long)i * n + cell, fn[i], i);
+    return kind == 2;
+}
+
+template <class S, int OP, bool SMAG, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+    k_step_tma(const StepArgs a, const __grid_constant__ CUtensorMap map) {
+    using T = typename S::T;
+    constexpr int XPAD = tma_xpad(sizeof(T));
+    constexpr int BX = tma_box_x(sizeof(T));
+    constexpr uint32_t BOX_BYTES = (uint32_t)(BX * TMA_BOX_Y * sizeof(T));
+    constexpr uint32_t STAGE = (uint32_t)tma_stage_bytes(sizeof(T));
+    extern __shared__ unsigned char tma_raw[];
+    const uint32_t raw = tc::smem_addr(tma_raw);
+    const uint32_t base = (raw + 127u) & ~127u;  // barriers at base, stages from base + 128
+    const T *stage_ptr = reinterpret_cast<const T *>(tma_raw + (base - raw) + 128);
+    const uint32_t bar[2] = {base, base + 8};
+
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const bool leader = tx == 0 && ty == 0;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * TMA_BOX_Y;
+    const int x = x0 + tx, y = y0 + ty;
+    const int zb = blockIdx.z * TMA_ZSEG;
+    const int ze = min(zb + TMA_ZSEG, a.nz);
+    const int zs = max(zb, 1), zt = min(ze, a.nz - 1);  // staged planes [zs, zt)
+    const int K = zt > zs ? zt - zs : 0;
+    const bool inside = x < a.nx && y < a.ny;
+    const bool interior = x > 0 && x + 1 < a.nx && y > 0 && y + 1 < a.ny;
+    const int col = ty * BX + tx + XPAD;
+    int resets = 0;
+
+    auto issue = [&](int k) {
+        const int z = zs + k;
+        const uint32_t b = bar[k & 1];
+        const uint32_t dst = base + 128 + (uint32_t)(k & 1) * STAGE;
+        tc::mbar_arrive_expect_tx(b, STAGE);
+#pragma unroll
+        for (int i = 0; i < 19; i++)
+            tc::tma_load_4d(dst + (uint32_t)i * BOX_BYTES, &map, x0 - XPAD, y0 - cy(i), z - cz(i),
+                            i, b);
+    };
+
+    if (leader && K > 0) {
+        tc::mbar_init(bar[0], 1);
+        tc::mbar_init(bar[1], 1);
+        tc::mbar_init_fence();
+        issue(0);
+        if (K > 1) issue(1);
+    }
+    __syncthreads();
+
+    // One pass over the segment's planes; the planes on the z edges of the
+    // grid (outside [zs, zt)) take the direct path.
+    bool tma_ok = true;  // block-uniform
+    int failed_at = K;   // first plane whose wait gave up
+#pragma unroll 1
+    for (int z = zb; z < ze; z++) {
+        const int k = z - zs;
+        const bool stage_plane = k >= 0 && k < K;
+        bool staged = false;
+        if (stage_plane && tma_ok) {
+            const bool got = tc::mbar_wait(bar[k & 1], (uint32_t)(k >> 1) & 1u, TMA_WAIT_LIMIT);
+            tma_ok = __syncthreads_and(got) != 0;
+            staged = tma_ok;
+            if (!tma_ok) {
+                failed_at = k;
+                if (leader && a.err) atomicOr(a.err, 1);
+            }
+        }
+        if (inside)
+            resets += tma_cell<S, OP, SMAG>(a, stage_ptr + (k & 1) * (STAGE / sizeof(T)),
+                                            staged && interior, x, y, z, col);
+        if (staged && k + 2 < K) {
+            __syncthreads();  // every thread is done with stage k & 1
+            if (leader) issue(k + 2);
+        }
+    }
+    if (!tma_ok && leader) {
+        // let the copies still in flight (planes failed_at and the next one)
+        // land before the block exits
+        for (int k = failed_at; k < K && k < failed_at + 2; k++)
+            tc::mbar_wait(bar[k & 1], (uint32_t)(k >> 1) & 1u, TMA_WAIT_LIMIT);
+    }
+
+    const unsigned any = __ballot_sync(0xffffffffu, resets > 0);
+    if (any) {
+        int v = resets;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (tx == 0 && v) atomicAdd(a.guard, (unsigned long long)v);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Batched step: one launch advances up to BATCH_LAUNCH_MAX grids by one
 // fused step.  Work unit: a column of up to BATCH_ZB consecutive z-planes of
 // one 256-cell tile, one 256-thread block per unit; the block finds its grid
@@ -432,10 +569,26 @@ struct StepLaunch {
         return dim3((wx + g.bx - 1) / g.bx, (g.ny + g.by - 1) / g.by, g.nz);
     }
 
+    // whether a fused step of this grid runs k_step_tma
+    static bool use_tma(const GridImpl &g, const StepArgs &a) {
+        return sizeof(typename S::T) <= 4 && g.tma && g.bx == 32 && g.by == TMA_BOX_Y &&
+               g.cpt == 1 && (a.src == g.pop[0] || a.src == g.pop[1]);
+    }
+
     template <int OP, bool SMAG>
     static void go(const GridImpl &g, const StepArgs &a, bool fused, cudaStream_t s) {
         const dim3 blk(g.bx, g.by, 1);
         const int cpt = (g.cpt == 2 && g.nx % 2 == 0) ? 2 : 1;
+        if constexpr (sizeof(typename S::T) <= 4) {
+            if (fused && use_tma(g, a)) {
+                const dim3 grd((g.nx + 31) / 32, (g.ny + TMA_BOX_Y - 1) / TMA_BOX_Y,
+                               (g.nz + TMA_ZSEG - 1) / TMA_ZSEG);
+                k_step_tma<S, OP, SMAG, 4><<<grd, dim3(32, TMA_BOX_Y, 1),
+                                             tma_smem_bytes(sizeof(typename S::T)), s>>>(
+                    a, g.tmap[a.src == g.pop[0] ? 0 : 1]);
+                return;
+            }
+        }
         if (fused) {
             if (cpt == 2)
                 k_step<S, OP, SMAG, true, 2, 1><<<grid3(g, 2), blk, 0, s>>>(a);
@@ -459,6 +612,28 @@ struct StepLaunch {
             default: go<OP_MRT, true>(g, a, fused, s); break;
         }
         return cudaGetLastError();
+    }
+
+    // Allow k_step_tma's dynamic shared memory for every operator.
+    static cudaError_t tma_prepare() {
+        if constexpr (sizeof(typename S::T) <= 4) {
+            const int bytes = tma_smem_bytes(sizeof(typename S::T));
+            cudaError_t e = cudaSuccess;
+            auto set = [&](const void *fn) {
+                if (e == cudaSuccess)
+                    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             bytes);
+            };
+            set((const void *)k_step_tma<S, OP_BGK, false, 4>);
+            set((const void *)k_step_tma<S, OP_BGK, true, 4>);
+            set((const void *)k_step_tma<S, OP_REG, false, 4>);
+            set((const void *)k_step_tma<S, OP_REG, true, 4>);
+            set((const void *)k_step_tma<S, OP_MRT, false, 4>);
+            set((const void *)k_step_tma<S, OP_MRT, true, 4>);
+            return e;
+        } else {
+            return cudaErrorNotSupported;
+        }
     }
 
     static cudaError_t stream_only(const GridImpl &g, const StepArgs &a, cudaStream_t s) {

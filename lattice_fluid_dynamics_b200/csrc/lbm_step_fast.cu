@@ -18,5 +18,14 @@ cudaError_t launch_step_fast(const GridImpl &g, const StepArgs &a, bool fused, i
     }
 }
 
+cudaError_t tma_prepare_fast(int storage) {
+    switch (storage) {
+        case LBM_STORAGE_FP32: return StepLaunch<StoreF32>::tma_prepare();
+        case LBM_STORAGE_FP16: return StepLaunch<StoreF16>::tma_prepare();
+        case LBM_STORAGE_BF16: return StepLaunch<StoreBF16>::tma_prepare();
+        default: return cudaErrorNotSupported;
+    }
+}
+
 }  // namespace fast
 }  // namespace lbm

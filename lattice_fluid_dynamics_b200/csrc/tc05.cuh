@@ -1,5 +1,6 @@
-// Thin wrappers over the sm_100a tensor-core (tcgen05) and mbarrier
-// instructions used by the warm-start network's GEMM kernels.
+// Thin wrappers over the sm_100a tensor-core (tcgen05), tensor-memory-access
+// (TMA) and mbarrier instructions used by the warm-start network's GEMM
+// kernels and the TMA-staged step kernel.
 //
 // Operands live in shared memory in the K-major "no swizzle" canonical
 // layout: 8 x 16-byte core matrices (8 rows of 8 bf16 along K), the core
@@ -60,6 +61,30 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_
         if (done) return true;
     }
     return false;
+}
+
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Arrive on the barrier and add `bytes` to the transaction count its current
+// phase waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// TMA load (no multicast) of one box of a rank-4 tensor map in this GPU's
+// memory into this CTA's shared memory, completing its bytes on the barrier.
+// The innermost coordinate times the element size must be a multiple of 16
+// bytes.
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const void *map, int c0, int c1, int c2,
+                                            int c3, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
 }
 
 // Generic-proxy shared-memory writes become visible to the tensor core.
