@@ -62,7 +62,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
 void setup_tma(GridImpl &g, bool force) {
     g.tma = false;
     const char *env = getenv("LBM_TMA");
-    if (!force && env && atoi(env) == 0) return;
+    if (!force && !(env && atoi(env) == 1)) return;
     CUtensorMapDataType dt;
     switch (g.storage) {
         case LBM_STORAGE_FP32: dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT32; break;

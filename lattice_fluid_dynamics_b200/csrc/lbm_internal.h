@@ -176,7 +176,7 @@ cudaError_t tma_prepare_fast(int storage);
 }
 // Encode the grid's TMA descriptors and allow k_step_tma's shared memory;
 // sets g.tma (false for FP64 storage or rows that are not a multiple of 16
-// bytes, or, unless `force`, when LBM_TMA=0 is set in the environment).
+// bytes, and, unless `force`, unless LBM_TMA=1 is set in the environment).
 void setup_tma(GridImpl &g, bool force);
 cudaError_t launch_stream_only(const GridImpl &g, const void *src, void *dst, int periodic,
                                cudaStream_t s);
