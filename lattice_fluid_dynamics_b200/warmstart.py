@@ -238,19 +238,31 @@ VARIANTS = {
 
 def evaluate(net: capi.WarmNet, shapes, dims=(256, 128, 128), sample: int = 50,
              cold_steps: int = 30000, avg_steps: int = 2000, ref_steps: int = 5000,
-             hold_steps: int = 5000, variants=("warm_fp16",)):
+             hold_steps: int = 5000, variants=("warm_fp16",), fp16_reference: bool = False):
     """Per shape: the converged Cd (mean of the raw Cd over the last
     ref_steps of a cold FP32 run of cold_steps) and, for the cold FP32 run
     and every variant, the steps and wall time until the Cd averaged over the
     trailing avg_steps enters and stays within 0.5 % of it (a variant's run
     stops once it has stayed in the band for hold_steps).  Warm variants fall
     back to uniform flow when the warm-started run trips the stability guard
-    or its drag is not finite."""
+    or its drag is not finite.
+
+    With fp16_reference, a cold FP16-storage run of cold_steps gives a second
+    converged Cd (its own, `cd_ref16`, row "cold_fp16_ref"), and every
+    FP16-storage variant also reports the steps and wall time to the band
+    around that value ("steps16", "wall_s16"): warm vs uniform start with
+    FP16 storage on, each judged against the FP16 cold start's converged Cd.
+    Those variants then run until they have held both bands."""
     import torch
     rows = []
     w = max(1, avg_steps // sample)
     hold = max(1, hold_steps // sample)
     L = capi.load()
+
+    def held(cds, ref):
+        e = entry_index(smoothed(cds, w), ref)
+        return e is not None and len(cds) - e >= hold
+
     for s in shapes:
         U = s["U"]
         g = make_grid(s, dims, "fp32")
@@ -271,14 +283,35 @@ def evaluate(net: capi.WarmNet, shapes, dims=(256, 128, 128), sample: int = 50,
                              "guard_resets": cold_resets,
                              "series": [round(v, 5) for v in smoothed(cd_c, w)[::10]]}}
 
-        def stop(cds):
-            if len(cds) < w:
-                return False
-            e = entry_index(smoothed(cds, w), ref)
-            return e is not None and len(cds) - e >= hold
+        ref16 = None
+        if fp16_reference:
+            g = make_grid(s, dims, "fp16")
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            g.initialize_flow(U)
+            init16 = time.perf_counter() - t0
+            cd_h, t_h = _run(g, U, area, sample, cold_steps)
+            resets16 = g.guard_resets()
+            g.close()
+            ref16 = float(np.mean(cd_h[-max(1, ref_steps // sample):]))
+            ih = entry_index(smoothed(cd_h, w), ref16)
+            row["cd_ref16"] = ref16
+            row["cold_fp16_ref"] = {
+                "steps": None if ih is None else (ih + 1) * sample,
+                "wall_s": None if ih is None else init16 + t_h[ih],
+                "ms_per_step": 1e3 * t_h[-1] / (len(t_h) * sample),
+                "guard_resets": resets16,
+                "series": [round(v, 5) for v in smoothed(cd_h, w)[::10]]}
 
         for name in variants:
             storage, init = VARIANTS[name]
+            use16 = ref16 is not None and storage.startswith("fp16")
+
+            def stop(cds):
+                if len(cds) < w:
+                    return False
+                return held(cds, ref) and (not use16 or held(cds, ref16))
+
             g = make_grid(s, dims, storage)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -306,6 +339,10 @@ def evaluate(net: capi.WarmNet, shapes, dims=(256, 128, 128), sample: int = 50,
                          "ms_per_step": 1e3 * t_v[-1] / (len(t_v) * sample),
                          "cd_end": float(np.mean(cd_v[-w:])),
                          "series": [round(v, 5) for v in smoothed(cd_v, w)[::10]]}
+            if use16:
+                i16 = entry_index(smoothed(cd_v, w), ref16)
+                row[name]["steps16"] = None if i16 is None else (i16 + 1) * sample
+                row[name]["wall_s16"] = None if i16 is None else t_init + t_v[i16]
         rows.append(row)
     return rows
 
@@ -322,6 +359,31 @@ def summarize(rows, variant="warm_fp16"):
     vs = np.array([r[variant]["steps"] for r in ok], float)
     ct = np.array([r["cold_fp32"]["wall_s"] for r in ok], float)
     vt = np.array([r[variant]["wall_s"] for r in ok], float)
+    out.update({
+        "cold_steps_median": float(np.median(cs)), "steps_median": float(np.median(vs)),
+        "cold_wall_s_median": float(np.median(ct)), "wall_s_median": float(np.median(vt)),
+        "wall_ratio_median": float(np.median(vt / ct)),
+        "wall_ratio_total": float(vt.sum() / ct.sum()),
+        "steps_ratio_total": float(vs.sum() / cs.sum()),
+        "faster_fraction": float(np.mean(vt < ct)),
+    })
+    return out
+
+
+def summarize_fp16(rows, variant="warmc_fp16"):
+    """The same medians and totals for an FP16-storage variant against the
+    cold FP16 start, both judged by the band around the cold FP16 start's
+    own converged Cd (rows made with fp16_reference)."""
+    ok = [r for r in rows if r.get("cold_fp16_ref", {}).get("steps")
+          and r.get(variant, {}).get("steps16")]
+    out = {"variant": variant, "baseline": "cold_fp16_ref", "evaluated": len(rows),
+           "both_converged": len(ok)}
+    if not ok:
+        return out
+    cs = np.array([r["cold_fp16_ref"]["steps"] for r in ok], float)
+    vs = np.array([r[variant]["steps16"] for r in ok], float)
+    ct = np.array([r["cold_fp16_ref"]["wall_s"] for r in ok], float)
+    vt = np.array([r[variant]["wall_s16"] for r in ok], float)
     out.update({
         "cold_steps_median": float(np.median(cs)), "steps_median": float(np.median(vs)),
         "cold_wall_s_median": float(np.median(ct)), "wall_s_median": float(np.median(vt)),
@@ -393,6 +455,8 @@ def main(argv=None) -> int:
     ap.add_argument("--scaling", default="", help="results .json holding the output scaling")
     ap.add_argument("--bench-train", type=int, default=0,
                     help="only time this many training steps on synthetic data")
+    ap.add_argument("--fp16-reference", action="store_true",
+                    help="also judge FP16 variants against a cold FP16 run's converged Cd")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     if a.bench_train:
@@ -413,9 +477,16 @@ def main(argv=None) -> int:
     # held-out shapes: indices beyond the training and validation ones
     shapes = [random_union(a.seed, 100000 + i) for i in range(a.eval)]
     variants = tuple(a.variants.split(","))
-    rows = evaluate(net, shapes, full, a.sample, a.cold_steps, variants=variants)
+    rows = evaluate(net, shapes, full, a.sample, a.cold_steps, variants=variants,
+                    fp16_reference=a.fp16_reference)
     res["rows"] = rows
+    if a.out:  # the rows first: they hold everything the summaries are made from
+        with open(a.out, "w") as fh:
+            json.dump(res, fh)
     res["summary"] = {v: summarize(rows, v) for v in variants}
+    if a.fp16_reference:
+        res["summary_fp16_reference"] = {
+            v: summarize_fp16(rows, v) for v in variants if VARIANTS[v][0].startswith("fp16")}
     print(json.dumps({k: v for k, v in res.items() if k not in ("rows", "history")} |
                      {"final": hist[-1] if hist else None}))
     if a.out:

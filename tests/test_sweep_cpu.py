@@ -58,3 +58,27 @@ def test_warmstart_shapes_closed_disjoint_deterministic():
         assert 0.04 <= a["U"] <= 0.08 and 20 <= a["Re"] <= 100
     assert not np.array_equal(ws.random_union(2, 0)["triangles"],
                               ws.random_union(2, 100000)["triangles"])
+
+
+def test_warmstart_entry_and_summaries():
+    from lattice_fluid_dynamics_b200 import warmstart as W
+    # trailing mean and the first sample after which it stays in the band
+    avg = W.smoothed([1.0, 1.0, 2.0, 2.0, 2.0], 2)
+    assert np.allclose(avg, [1.0, 1.0, 1.5, 2.0, 2.0])
+    assert W.entry_index(avg, 2.0) == 3
+    assert W.entry_index(avg, 2.0, band=0.3) == 2
+    assert W.entry_index([1.0, 1.0, 3.0], 1.0) is None   # leaves the band at the end
+    assert W.entry_index([1.0, 1.0], 1.0) == 0
+    rows = [
+        {"cold_fp32": {"steps": 4000, "wall_s": 0.4}, "cold_fp16_ref": {"steps": 3000, "wall_s": 0.3},
+         "warmc_fp16": {"steps": None, "wall_s": None, "steps16": 1000, "wall_s16": 0.1}},
+        {"cold_fp32": {"steps": 9000, "wall_s": 0.9}, "cold_fp16_ref": {"steps": 8000, "wall_s": 0.8},
+         "warmc_fp16": {"steps": 2000, "wall_s": 0.2, "steps16": 2000, "wall_s16": 0.2}},
+    ]
+    s32 = W.summarize(rows, "warmc_fp16")
+    assert s32["both_converged"] == 1 and s32["wall_ratio_total"] == 0.2 / 0.9
+    s16 = W.summarize_fp16(rows, "warmc_fp16")
+    assert s16["both_converged"] == 2
+    assert abs(s16["wall_ratio_total"] - 0.3 / 1.1) < 1e-12
+    assert s16["steps_ratio_total"] == 3000 / 11000
+    assert s16["faster_fraction"] == 1.0
