@@ -313,11 +313,13 @@ class Grid:
             self._L.LBM_Step(self._g, ux, uy, uz)
 
     def drag_force_decomposed(self) -> np.ndarray:
-        out = (C.c_float * 6)()
-        self._L.LBM_ComputeDragForceDecomposed(
-            self._g, *[C.addressof(out) + 4 * k for k in range(6)])
+        if getattr(self, "_fout", None) is None:  # one output block per grid
+            self._fout = np.zeros(6, np.float32)
+            base = self._fout.ctypes.data
+            self._fptr = [base + 4 * k for k in range(6)]
+        self._L.LBM_ComputeDragForceDecomposed(self._g, *self._fptr)
         self.check()
-        return np.frombuffer(out, np.float32).copy()
+        return self._fout.copy()
 
     def drag_force_f64(self):
         out = np.zeros(6, np.float64)

@@ -316,8 +316,10 @@ LBMGrid *LBM_CreateEx(int sizeX, int sizeY, int sizeZ, float viscosity, int stor
     good = good && ok(grid, cudaMalloc(&I->solid, sizeof(int32_t) * (size_t)n));
     good = good && ok(grid, cudaMalloc(&I->flags, (size_t)n));
     good = good && ok(grid, cudaMalloc(&I->slot, sizeof(int32_t) * (size_t)n));
-    good = good && ok(grid, cudaMalloc(&I->force_i64, sizeof(long long) * 8));
-    good = good && ok(grid, cudaMalloc(&I->force_f64, sizeof(double) * 8));
+    // one block: 8 integer sums, then 8 FP64 sums, zeroed and read back
+    // with one call each
+    good = good && ok(grid, cudaMalloc(&I->force_i64, sizeof(long long) * 16));
+    if (good) I->force_f64 = reinterpret_cast<double *>(I->force_i64 + 8);
     good = good && ok(grid, cudaMalloc(&I->sums_f64, sizeof(double) * 4));
     good = good && ok(grid, cudaMalloc(&I->guard, sizeof(unsigned long long)));
     good = good && ok(grid, cudaMalloc(&I->err_flag, sizeof(int)));
@@ -364,8 +366,7 @@ void LBM_Free(LBMGrid *grid) {
         cudaFree(I->solid);
         cudaFree(I->flags);
         cudaFree(I->slot);
-        cudaFree(I->force_i64);
-        cudaFree(I->force_f64);
+        cudaFree(I->force_i64);  // force_f64 lives in the same block
         cudaFree(I->sums_f64);
         cudaFree(I->guard);
         cudaFree(I->err_flag);
@@ -625,10 +626,8 @@ int LBM_ComputeDragForceF64(LBMGrid *grid, double *out6, long long *raw7) {
     bool good = ok(grid, launch_force(*I, I->pop[I->gbuf], fexp, I->stream_periodic, vel,
                                       I->vel64, I->pop[I->vin], I->vin_kind, I->vin_periodic, I->vin_inlet,
                                       I->force_i64, I->force_f64, I->stream));
-    long long *h = I->host_pinned;
-    good = good && ok(grid, cudaMemcpyAsync(h, I->force_i64, sizeof(long long) * 7,
-                                            cudaMemcpyDeviceToHost, I->stream));
-    good = good && ok(grid, cudaMemcpyAsync(h + 8, I->force_f64, sizeof(double) * 6,
+    long long *h = I->host_pinned;  // h[0..6] integer sums, h[8..13] FP64 sums
+    good = good && ok(grid, cudaMemcpyAsync(h, I->force_i64, sizeof(long long) * 14,
                                             cudaMemcpyDeviceToHost, I->stream));
     good = good && sync(grid);
     if (!good) return 0;

@@ -194,9 +194,13 @@ cudaError_t launch_force(const GridImpl &g, const void *gsrc, const void *f_expl
                          const void *vin_src,
                          int vin_kind, int vin_periodic, const float vin_inlet[3],
                          long long *i64, double *f64, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(i64, 0, sizeof(long long) * 7, s);
-    if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(f64, 0, sizeof(double) * 6, s);
+    cudaError_t e;
+    if (reinterpret_cast<void *>(f64) == reinterpret_cast<void *>(i64 + 8)) {
+        e = cudaMemsetAsync(i64, 0, sizeof(long long) * 14, s);  // one block
+    } else {
+        e = cudaMemsetAsync(i64, 0, sizeof(long long) * 7, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(f64, 0, sizeof(double) * 6, s);
+    }
     if (e != cudaSuccess) return e;
     ForceArgs a{};
     a.st.src = gsrc;

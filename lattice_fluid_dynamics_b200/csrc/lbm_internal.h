@@ -55,8 +55,8 @@ struct GridImpl {
     int32_t *slot = nullptr;            // boundary-cell index or -1
     LinkList links;
 
-    long long *force_i64 = nullptr;     // [7]
-    double *force_f64 = nullptr;        // [6]
+    long long *force_i64 = nullptr;     // [7] of a 16-slot block
+    double *force_f64 = nullptr;        // [6], slots 8.. of the same block
     double *sums_f64 = nullptr;         // [4]
     unsigned long long *guard = nullptr;  // cumulative guard resets
     int *err_flag = nullptr;            // device-side error word
