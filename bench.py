@@ -321,7 +321,7 @@ def main():
                          "bytes_per_update": bpu},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_mlups, 2), "unit": "MLUPS", "steps": ke,
-                    "h2d_bytes_per_step": 12, "d2h_bytes_per_step": 7 * 8 + 6 * 8},
+                    "h2d_bytes_per_step": 12, "d2h_bytes_per_step": 14 * 8},
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
             "cd_last": round(cds[-1], 5) if cds else None,
