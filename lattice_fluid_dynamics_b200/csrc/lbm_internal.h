@@ -120,6 +120,15 @@ struct StepArgs {
     int *err;          // device error word (bit 0: a TMA wait gave up)
 };
 
+// Per-launch element offsets of the fused step, computed on the host so
+// that every address is a per-thread base plus a kernel-parameter constant:
+// pull[i] = i*n - e_ix - e_iy*NX - e_iz*NX*NY (the pulled neighbour of an
+// interior cell in plane i), dir[i] = i*n (plane i of the cell itself).
+struct StepOffsets {
+    long long pull[19];
+    long long dir[19];
+};
+
 // One grid of a batched step launch (k_step_batch): its step arguments,
 // operator, and tile shape -- 1 << lbx cells along x (32..256) by
 // 256 >> lbx rows, tiles_x * tiles_y tiles per z plane.

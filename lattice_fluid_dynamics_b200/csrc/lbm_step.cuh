@@ -74,8 +74,8 @@ __device__ __forceinline__ void gather_pull(const StepArgs &a, const typename S:
 // are all inside the grid: every direction reads at a warp-uniform offset
 // from the cell, and the directions with e_x == 0 read both cells with one
 // aligned pair load.
-template <class S, int CPT>
-__device__ __forceinline__ void gather_interior(const StepArgs &a,
+template <class S, int CPT, bool TAB>
+__device__ __forceinline__ void gather_interior(const StepArgs &a, const long long *pull,
                                                 const typename S::T *__restrict__ src,
                                                 long long cell0, typename S::R (&f0)[19],
                                                 typename S::R (&f1)[19]) {
@@ -83,7 +83,8 @@ __device__ __forceinline__ void gather_interior(const StepArgs &a,
     const long long n = a.n, nx = a.nx, plane = (long long)a.nx * a.ny;
 #pragma unroll
     for (int i = 0; i < 19; i++) {
-        const long long off = (long long)i * n - cx(i) - cy(i) * nx - cz(i) * plane;
+        const long long off =
+            TAB ? pull[i] : (long long)i * n - cx(i) - cy(i) * nx - cz(i) * plane;
         if (CPT == 2 && cx(i) == 0) {
             S::load2(p + off, i, f0[i], f1[i]);
         } else {
@@ -167,8 +168,12 @@ __device__ __forceinline__ int collide_cell(const StepArgs &a, typename S::R (&f
 // One thread's share of a step: CPT cells starting at (x0, y, z).  CPT =
 // cells per thread along x (1 or 2; 2 needs an even NX).  `lane` is the
 // thread's lane in its warp (for the warp-aggregated guard count).
-template <class S, int OP, bool SMAG, bool FUSED, int CPT>
-__device__ __forceinline__ void step_cells(const StepArgs &a, int x0, int y, int z) {
+// TAB: take the interior pull offsets and the plane offsets from a
+// StepOffsets kernel parameter (`o`, ignored otherwise) instead of deriving
+// them from the grid sizes.
+template <class S, int OP, bool SMAG, bool FUSED, int CPT, bool TAB = false>
+__device__ __forceinline__ void step_cells(const StepArgs &a, const StepOffsets *o, int x0, int y,
+                                           int z) {
     using T = typename S::T;
     using R = typename S::R;
     if (x0 >= a.nx || y >= a.ny) return;
@@ -192,7 +197,7 @@ __device__ __forceinline__ void step_cells(const StepArgs &a, int x0, int y, int
         const bool interior = x0 > 0 && x0 + CPT < a.nx && y > 0 && y + 1 < a.ny && z > 0 &&
                               z + 1 < a.nz;
         if (interior) {
-            gather_interior<S, CPT>(a, src, cell0, cur, nxt);
+            gather_interior<S, CPT, TAB>(a, TAB ? o->pull : nullptr, src, cell0, cur, nxt);
         } else {
             const Rows rw = neighbour_rows(a, y, z);
             gather_pull<S>(a, src, x0, rw, cell0, cur);
@@ -224,10 +229,11 @@ __device__ __forceinline__ void step_cells(const StepArgs &a, int x0, int y, int
         if (c == CPT - 1) {
 #pragma unroll
             for (int i = 0; i < 19; i++) {
+                const long long plane_i = TAB ? o->dir[i] : (long long)i * n;
                 if (CPT == 2)
-                    S::store2(dst + (long long)i * n + cell0, keep[i], fn[i], i);
+                    S::store2(dst + plane_i + cell0, keep[i], fn[i], i);
                 else
-                    S::store(dst + (long long)i * n + cell0, fn[i], i);
+                    S::store(dst + plane_i + cell0, fn[i], i);
             }
         } else {
 #pragma unroll
@@ -248,10 +254,22 @@ __device__ __forceinline__ void step_cells(const StepArgs &a, int x0, int y, int
 }
 
 // The step over one grid: a 2D block tile of (bx * CPT) x by cells per z.
+// Whether k_step takes its offsets from the StepOffsets table.  Measured on
+// B200 at 256x128x128: +2.5 % for exact FP32 MRT + Smagorinsky (issue-bound,
+// and the table frees the registers that held the derived offsets), -1 to
+// -2 % for FP32 BGK / regularized / MRT, -8 to -9 % for FP16 BGK and
+// regularized; so only FP32 MRT + Smagorinsky uses it.
+template <class S, int OP, bool SMAG>
+__host__ __device__ constexpr bool step_offset_table() {
+    return sizeof(typename S::T) == 4 && OP == OP_MRT && SMAG;
+}
+
 template <class S, int OP, bool SMAG, bool FUSED, int CPT, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_step(const StepArgs a) {
-    step_cells<S, OP, SMAG, FUSED, CPT>(a, (blockIdx.x * blockDim.x + threadIdx.x) * CPT,
-                                        blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z);
+__global__ void __launch_bounds__(256, MINB)
+    k_step(const StepArgs a, const __grid_constant__ StepOffsets o) {
+    constexpr bool TAB = step_offset_table<S, OP, SMAG>();
+    step_cells<S, OP, SMAG, FUSED, CPT, TAB>(a, &o, (blockIdx.x * blockDim.x + threadIdx.x) * CPT,
+                                             blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -420,12 +438,12 @@ __global__ void __launch_bounds__(256, 4) k_step_batch(const __grid_constant__ B
     constexpr unsigned M = batch_set_mask(SET);
     auto cells = [&](int z) {
         switch (e.combo) {
-            case 0: if constexpr ((M & 1u) != 0) step_cells<S, OP_BGK, false, true, 1>(e.a, x, y, z); break;
-            case 1: if constexpr ((M & 2u) != 0) step_cells<S, OP_BGK, true, true, 1>(e.a, x, y, z); break;
-            case 2: if constexpr ((M & 4u) != 0) step_cells<S, OP_REG, false, true, 1>(e.a, x, y, z); break;
-            case 3: if constexpr ((M & 8u) != 0) step_cells<S, OP_REG, true, true, 1>(e.a, x, y, z); break;
-            case 4: if constexpr ((M & 16u) != 0) step_cells<S, OP_MRT, false, true, 1>(e.a, x, y, z); break;
-            default: if constexpr ((M & 32u) != 0) step_cells<S, OP_MRT, true, true, 1>(e.a, x, y, z); break;
+            case 0: if constexpr ((M & 1u) != 0) step_cells<S, OP_BGK, false, true, 1>(e.a, nullptr, x, y, z); break;
+            case 1: if constexpr ((M & 2u) != 0) step_cells<S, OP_BGK, true, true, 1>(e.a, nullptr, x, y, z); break;
+            case 2: if constexpr ((M & 4u) != 0) step_cells<S, OP_REG, false, true, 1>(e.a, nullptr, x, y, z); break;
+            case 3: if constexpr ((M & 8u) != 0) step_cells<S, OP_REG, true, true, 1>(e.a, nullptr, x, y, z); break;
+            case 4: if constexpr ((M & 16u) != 0) step_cells<S, OP_MRT, false, true, 1>(e.a, nullptr, x, y, z); break;
+            default: if constexpr ((M & 32u) != 0) step_cells<S, OP_MRT, true, true, 1>(e.a, nullptr, x, y, z); break;
         }
     };
     if constexpr (BATCH_ZB == 1) {
@@ -589,15 +607,21 @@ struct StepLaunch {
                 return;
             }
         }
+        StepOffsets o;
+        const long long plane = (long long)a.nx * a.ny;
+        for (int i = 0; i < 19; i++) {
+            o.dir[i] = (long long)i * a.n;
+            o.pull[i] = o.dir[i] - cx(i) - cy(i) * (long long)a.nx - cz(i) * plane;
+        }
         if (fused) {
             if (cpt == 2)
-                k_step<S, OP, SMAG, true, 2, 1><<<grid3(g, 2), blk, 0, s>>>(a);
+                k_step<S, OP, SMAG, true, 2, 1><<<grid3(g, 2), blk, 0, s>>>(a, o);
             else if (g.minb == 4)
-                k_step<S, OP, SMAG, true, 1, 4><<<grid3(g, 1), blk, 0, s>>>(a);
+                k_step<S, OP, SMAG, true, 1, 4><<<grid3(g, 1), blk, 0, s>>>(a, o);
             else
-                k_step<S, OP, SMAG, true, 1, 1><<<grid3(g, 1), blk, 0, s>>>(a);
+                k_step<S, OP, SMAG, true, 1, 1><<<grid3(g, 1), blk, 0, s>>>(a, o);
         } else {
-            k_step<S, OP, SMAG, false, 1, 1><<<grid3(g, 1), blk, 0, s>>>(a);
+            k_step<S, OP, SMAG, false, 1, 1><<<grid3(g, 1), blk, 0, s>>>(a, o);
         }
     }
 
