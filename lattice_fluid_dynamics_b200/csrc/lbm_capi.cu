@@ -319,7 +319,10 @@ LBMGrid *LBM_CreateEx(int sizeX, int sizeY, int sizeZ, float viscosity, int stor
     // one block: 8 integer sums, then 8 FP64 sums, zeroed and read back
     // with one call each
     good = good && ok(grid, cudaMalloc(&I->force_i64, sizeof(long long) * 16));
-    if (good) I->force_f64 = reinterpret_cast<double *>(I->force_i64 + 8);
+    if (good) {
+        I->force_f64 = reinterpret_cast<double *>(I->force_i64 + 8);
+        I->force_ticket = reinterpret_cast<unsigned *>(I->force_i64 + 15);
+    }
     good = good && ok(grid, cudaMalloc(&I->sums_f64, sizeof(double) * 4));
     good = good && ok(grid, cudaMalloc(&I->guard, sizeof(unsigned long long)));
     good = good && ok(grid, cudaMalloc(&I->err_flag, sizeof(int)));
@@ -335,6 +338,7 @@ LBMGrid *LBM_CreateEx(int sizeX, int sizeY, int sizeZ, float viscosity, int stor
         good = good && ok(grid, cudaMemsetAsync(I->slot, 0xff, sizeof(int32_t) * (size_t)n, s));
         good = good && ok(grid, cudaMemsetAsync(I->guard, 0, sizeof(unsigned long long), s));
         good = good && ok(grid, cudaMemsetAsync(I->err_flag, 0, sizeof(int), s));
+        good = good && ok(grid, cudaMemsetAsync(I->force_i64, 0, sizeof(long long) * 16, s));
         good = good && ok(grid, cudaStreamSynchronize(s));
     }
     if (!good) {
@@ -366,7 +370,8 @@ void LBM_Free(LBMGrid *grid) {
         cudaFree(I->solid);
         cudaFree(I->flags);
         cudaFree(I->slot);
-        cudaFree(I->force_i64);  // force_f64 lives in the same block
+        cudaFree(I->force_i64);  // force_f64 and force_ticket live in the same block
+        cudaFree(I->force_part);
         cudaFree(I->sums_f64);
         cudaFree(I->guard);
         cudaFree(I->err_flag);
@@ -623,9 +628,21 @@ int LBM_ComputeDragForceF64(LBMGrid *grid, double *out6, long long *raw7) {
     if (!I) return 0;
     const void *fexp = I->fbuf >= 0 ? I->pop[I->fbuf] : nullptr;
     const float4 *vel = I->vel_valid ? I->vel : nullptr;
+    const int blocks = force_blocks(I->links.nb);
+    if (blocks > I->force_part_blocks) {
+        // partial sums of the force kernel's blocks; grows with the link list
+        if (!ok(grid, cudaStreamSynchronize(I->stream))) return 0;
+        cudaFree(I->force_part);
+        I->force_part = nullptr;
+        I->force_part_blocks = 0;
+        if (!ok(grid, cudaMalloc(&I->force_part, sizeof(long long) * 16 * (size_t)blocks)))
+            return 0;
+        I->force_part_blocks = blocks;
+    }
     bool good = ok(grid, launch_force(*I, I->pop[I->gbuf], fexp, I->stream_periodic, vel,
                                       I->vel64, I->pop[I->vin], I->vin_kind, I->vin_periodic, I->vin_inlet,
-                                      I->force_i64, I->force_f64, I->stream));
+                                      I->force_i64, I->force_f64, I->force_part, I->force_ticket,
+                                      I->stream));
     long long *h = I->host_pinned;  // h[0..6] integer sums, h[8..13] FP64 sums
     good = good && ok(grid, cudaMemcpyAsync(h, I->force_i64, sizeof(long long) * 14,
                                             cudaMemcpyDeviceToHost, I->stream));

@@ -147,18 +147,6 @@ struct StoreBF16 {
     }
 };
 
-// ---------------------------------------------------------------------
-// Equilibrium (lbm_collide.comp:94-101, lbm_force.comp:216-221)
-// ---------------------------------------------------------------------
-template <typename R>
-__device__ __forceinline__ R feq(int i, R rho, R ux, R uy, R uz) {
-    R eu = R(cx(i)) * ux + R(cy(i)) * uy + R(cz(i)) * uz;
-    R u2 = ux * ux + uy * uy + uz * uz;
-    const R cs2 = R(1) / R(3);
-    return wgt<R>(i) * rho *
-           (R(1) + eu / cs2 + (eu * eu) / (R(2) * cs2 * cs2) - u2 / (R(2) * cs2));
-}
-
 template <typename R> __device__ __forceinline__ R dsqrt(R v);
 #ifdef LBM_FAST_ARITH
 template <> __device__ __forceinline__ float dsqrt<float>(float v) { return sqrtf(v); }
@@ -200,6 +188,24 @@ __device__ __forceinline__ float cdiv<float>(float x, float y, float zh) {
 template <>
 __device__ __forceinline__ double cdiv<double>(double x, double y, double) {
     return __ddiv_rn(x, y);
+}
+
+// Equilibrium (lbm_collide.comp:94-101, lbm_force.comp:216-221):
+// feq_i(rho, u) = w_i rho (1 + eu/cs2 + eu^2/(2 cs2^2) - u^2/(2 cs2))
+// evaluated in the reference's order (lbm.c:37-44).  The three quotients
+// are by the constants cs2, 2 cs2^2 and 2 cs2 and use cdiv, which equals
+// the IEEE quotient here: a numerator below 2^-100 gives a quotient that
+// 1 + ... absorbs either way.
+template <typename R>
+__device__ __forceinline__ R feq(int i, R rho, R ux, R uy, R uz) {
+    R eu = R(cx(i)) * ux + R(cy(i)) * uy + R(cz(i)) * uz;
+    R u2 = ux * ux + uy * uy + uz * uz;
+    constexpr R cs2 = R(1) / R(3);
+    constexpr R c2 = R(2) * cs2 * cs2;
+    constexpr R c1 = R(2) * cs2;
+    return wgt<R>(i) * rho *
+           (((R(1) + cdiv<R>(eu, cs2, R(1) / cs2)) + cdiv<R>(eu * eu, c2, R(1) / c2)) -
+            cdiv<R>(u2, c1, R(1) / c1));
 }
 
 // a*b + c with one rounding.  Used only where a is +-2, +-4 or +-8, so the

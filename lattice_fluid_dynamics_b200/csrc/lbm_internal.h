@@ -57,6 +57,9 @@ struct GridImpl {
 
     long long *force_i64 = nullptr;     // [7] of a 16-slot block
     double *force_f64 = nullptr;        // [6], slots 8.. of the same block
+    unsigned *force_ticket = nullptr;   // slot 15 of the same block
+    long long *force_part = nullptr;    // 16 slots per k_force block
+    int force_part_blocks = 0;
     double *sums_f64 = nullptr;         // [4]
     unsigned long long *guard = nullptr;  // cumulative guard resets
     int *err_flag = nullptr;            // device-side error word
@@ -221,7 +224,10 @@ cudaError_t launch_force(const GridImpl &g, const void *gsrc, const void *f_expl
                          int periodic, const float4 *vel_or_null, const double4 *vel64_or_null,
                          const void *vin_src,
                          int vin_kind, int vin_periodic, const float vin_inlet[3],
-                         long long *i64, double *f64, cudaStream_t s);
+                         long long *i64, double *f64, long long *part, unsigned *ticket,
+                         cudaStream_t s);
+// blocks of one k_force launch over nb boundary cells (16 partial slots each)
+int force_blocks(int nb);
 
 // lbm_particles.cu
 cudaError_t launch_particles(LBMParticle *p, int n, const float4 *vel, int nx, int ny, int nz,
