@@ -196,9 +196,10 @@ def reference_arm(args):
     if rank != 0:
         return 0
     budget = float(os.environ.get("LBM_REF_BUDGET_S", "60"))
-    mlups, steps, secs, cores = cpu_oracle_run(budget, max(args.steps, 2), warmup=min(args.warmup, 1))
+    warm = min(max(args.warmup, 3), 10)  # untimed CPU steps, bounded
+    mlups, steps, secs, cores = cpu_oracle_run(budget, max(args.steps, 2), warmup=warm)
     line = {"metric": "MLUPS", "value": round(mlups, 3), "unit": "MLUPS", "impl": "reference",
-            "n_gpus": world, "steps": steps, "warmup": min(args.warmup, 1),
+            "n_gpus": world, "steps": steps, "warmup": warm,
             "ms_per_step": round(1e3 * secs / steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config(world),
