@@ -117,7 +117,7 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # distributed plumbing (replicas)
 # ---------------------------------------------------------------------------
-def dist_setup(n_gpus: int):
+def dist_setup(n_gpus: int, backend: str | None = None):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -138,27 +138,41 @@ def dist_setup(n_gpus: int):
     if world > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if backend is None:  # one GPU per rank over NCCL; gloo on a host without GPUs
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         pg = dist
     return world, rank, phys, pg
+
+
+def _on_gpu(pg) -> bool:
+    return pg.get_backend() == "nccl"
 
 
 def barrier(pg):
     if pg is not None:
         import torch
-        t = torch.zeros(1, device="cuda")
+        t = torch.zeros(1, device="cuda" if _on_gpu(pg) else "cpu")
         pg.all_reduce(t)
-        torch.cuda.synchronize()
+        if _on_gpu(pg):
+            torch.cuda.synchronize()
 
 
 def max_over_ranks(pg, v: float) -> float:
     if pg is None:
         return v
     import torch
-    t = torch.tensor([v], device="cuda", dtype=torch.float64)
+    t = torch.tensor([v], device="cuda" if _on_gpu(pg) else "cpu", dtype=torch.float64)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_mlups(world: int, cells: int, steps: int, ms_max: float) -> float:
+    """Whole-job MLUPS of `world` replicas that each advanced `cells` by
+    `steps` steps, timed by the slowest rank (ms_max)."""
+    return world * cells * steps / (ms_max / 1e3) / 1e6
 
 
 # ---------------------------------------------------------------------------
@@ -292,8 +306,8 @@ def main():
     per_launch_s = ms_max / 1e3 / args.steps
     achieved = bpu * cells / per_launch_s / 1e9
     peak, peak_kind = peaks()
-    mlups = world * cells * args.steps / (ms_max / 1e3) / 1e6
-    e2e_mlups = world * cells * ke / (e2e_ms / 1e3) / 1e6
+    mlups = job_mlups(world, cells, args.steps, ms_max)
+    e2e_mlups = job_mlups(world, cells, ke, e2e_ms)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
