@@ -6,7 +6,10 @@ Each case makes a fresh grid, runs 64 untimed steps, then times `--steps`
 steps (LBM_StepN, CUDA graph chunks) with CUDA events on the grid's stream
 and prints one JSON line: MLUPS and GB/s of algorithmic population traffic.
 `--loop N` instead runs N single LBM_Step launches per case and no timing
-(a short target for a profiler).
+(a short target for a profiler).  `--readback K` adds K synchronous drag
+readbacks (LBM_ComputeDragForceDecomposed) per case; when timing, it reports
+the host time of one readback alone and of one LBM_Step + readback pair, the
+end-to-end loop of the reference's driver.
 
     python -m lattice_fluid_dynamics_b200.stepbench --storage fp16 --op bgk
     python -m lattice_fluid_dynamics_b200.stepbench --loop 3 --storage fp16 --op bgk
@@ -54,6 +57,24 @@ def timed(g: capi.Grid, steps: int) -> float:
     return e0.elapsed_time(e1)
 
 
+def readbacks(g: capi.Grid, k: int) -> dict:
+    """Host microseconds of one drag readback and of one LBM_Step + readback
+    (means over k; both are synchronous, so host time is the cost)."""
+    import time
+    g.drag_force_decomposed()
+    t0 = time.perf_counter()
+    for _ in range(k):
+        g.drag_force_decomposed()
+    t1 = time.perf_counter()
+    for _ in range(k):
+        g.step(U)
+        g.drag_force_decomposed()
+    t2 = time.perf_counter()
+    g.check()
+    return {"readback_us": round(1e6 * (t1 - t0) / k, 1),
+            "step_readback_us": round(1e6 * (t2 - t1) / k, 1)}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--dims", default="256x128x128")
@@ -64,6 +85,7 @@ def main(argv=None) -> int:
                     choices=["direct", "staged"])
     ap.add_argument("--steps", type=int, default=512)
     ap.add_argument("--loop", type=int, default=0)
+    ap.add_argument("--readback", type=int, default=0)
     args = ap.parse_args(argv)
     dims = tuple(int(v) for v in args.dims.split("x"))
     tris, bbox = geometry.ahmed_body()
@@ -77,6 +99,8 @@ def main(argv=None) -> int:
                                dims=list(dims))
                     if args.loop:
                         g.step_loop(U, n=args.loop)
+                        for _ in range(args.readback):
+                            g.drag_force_decomposed()
                         g.check()
                     else:
                         ms = timed(g, args.steps)
@@ -85,6 +109,8 @@ def main(argv=None) -> int:
                                    mlups=round(cells * args.steps / s / 1e6, 1),
                                    gb_per_s=round(cells * args.steps * g.bytes_per_update()
                                                   / s / 1e9, 1))
+                        if args.readback:
+                            row.update(readbacks(g, args.readback))
                     g.close()
                     print(json.dumps(row), flush=True)
     return 0
