@@ -251,7 +251,7 @@ def evaluate(net: capi.WarmNet, shapes, dims=(256, 128, 128), sample: int = 50,
     converged Cd (its own, `cd_ref16`, row "cold_fp16_ref"), and every
     FP16-storage variant also reports the steps and wall time to the band
     around that value ("steps16", "wall_s16"): warm vs uniform start with
-    FP16 storage on, each judged against the FP16 cold start's converged Cd.
+    FP16 storage on, each measured against the FP16 cold start's converged Cd.
     Those variants then run until they have held both bands."""
     import torch
     rows = []
@@ -456,7 +456,7 @@ def main(argv=None) -> int:
     ap.add_argument("--bench-train", type=int, default=0,
                     help="only time this many training steps on synthetic data")
     ap.add_argument("--fp16-reference", action="store_true",
-                    help="also judge FP16 variants against a cold FP16 run's converged Cd")
+                    help="also measure FP16 variants against a cold FP16 run's converged Cd")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     if a.bench_train:
