@@ -372,7 +372,7 @@ def summarize(rows, variant="warm_fp16"):
 
 def summarize_fp16(rows, variant="warmc_fp16"):
     """The same medians and totals for an FP16-storage variant against the
-    cold FP16 start, both judged by the band around the cold FP16 start's
+    cold FP16 start, both measured by the band around the cold FP16 start's
     own converged Cd (rows made with fp16_reference)."""
     ok = [r for r in rows if r.get("cold_fp16_ref", {}).get("steps")
           and r.get(variant, {}).get("steps16")]
