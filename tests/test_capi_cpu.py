@@ -62,3 +62,16 @@ def test_error_strings(solver):
     assert lib.LBM_GetErrorString(0) == b"ok"
     assert lib.LBM_GetErrorString(2) == b"out of device memory"
     assert lib.LBM_GetLastError(None) != 0
+
+
+def test_create_rejects_bad_sizes_before_any_device_call(solver):
+    # lbm.c:46-60 returns NULL on failure; sizes are checked on the host
+    # before any allocation: non-positive extents, more than 2^31 - 1 cells,
+    # an unknown storage format.  Freeing NULL is allowed (lbm.c:320-344).
+    from lattice_fluid_dynamics_b200 import capi
+    lib = capi.load()
+    for dims in [(0, 8, 8), (8, -1, 8), (8, 8, 0), (2048, 2048, 1024), (65536, 65536, 1)]:
+        assert not lib.LBM_CreateEx(*dims, 0.1, 0)
+        assert not lib.LBM_Create(*dims, 0.1)
+    assert not lib.LBM_CreateEx(8, 8, 8, 0.1, 99)
+    lib.LBM_Free(None)
