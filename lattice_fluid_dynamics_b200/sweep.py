@@ -13,11 +13,18 @@ its chosen tile, and -- with ``solo=True`` -- the same instances stepped one
 grid at a time (LBM_StepN), whose Cd must be identical.
 
     python -m lattice_fluid_dynamics_b200.sweep --count 64 --steps 3000
+
+Under torchrun (one process per GPU) every rank takes its share of the
+instances (``shard``: a near-equal number of lattice updates each), runs it
+as its own batch with no collective on the data path, and rank 0 gathers the
+per-instance results; the aggregate MLUPS counts every rank's updates over
+the slowest rank's time.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import os
 import sys
 import time
 
@@ -58,9 +65,53 @@ def _timed(stream_ptr: int, fn) -> float:
     return e0.elapsed_time(e1)
 
 
+def shard(dims, world: int, rank: int) -> list:
+    """Indices of the instances rank `rank` of `world` runs: largest grids
+    first, each to the rank with the fewest cells so far (ties: lowest
+    rank), so every rank gets a near-equal share of lattice updates."""
+    load = [0] * world
+    owner = [0] * len(dims)
+    sizes = [int(np.prod(d)) for d in dims]
+    for k in sorted(range(len(dims)), key=lambda k: (-sizes[k], k)):
+        r = min(range(world), key=lambda j: (load[j], j))
+        owner[k] = r
+        load[r] += sizes[k]
+    return [k for k in range(len(dims)) if owner[k] == rank]
+
+
+def merge_ranks(results: list) -> dict:
+    """One sweep result from the per-rank results of a sharded sweep: the
+    instances in index order, updates of every rank over the slowest rank's
+    time."""
+    first = results[0]
+    ms = max(r["ms"] for r in results)
+    cells = sum(r["cells_total"] for r in results)
+    total = cells * first["steps"]
+    out = {k: first[k] for k in ("steps", "seed", "storage")}
+    out.update({
+        "instances": sum(r["instances"] for r in results), "ranks": len(results),
+        "cells_total": cells, "ms": ms, "mlups": total / (ms * 1e-3) / 1e6,
+        "gb_per_s": sum(r["gb_per_s"] * r["ms"] for r in results) / ms,
+        "per_rank_ms": [r["ms"] for r in results],
+        "schedule": [r["schedule"] for r in results],
+        "per_instance": sorted((p for r in results for p in r["per_instance"]),
+                               key=lambda p: p["index"]),
+    })
+    if all("cd_identical" in r for r in results):
+        out["cd_identical"] = sum(r["cd_identical"] for r in results)
+    return out
+
+
 def run_sweep(count: int = 64, steps: int = 3000, seed: int = 1, autotune: bool = True,
-              solo: bool = True, storage: str = "fp32", warmup: int = 0) -> dict:
+              solo: bool = True, storage: str = "fp32", warmup: int = 0,
+              indices=None) -> dict:
+    """The sweep of `count` instances from `seed`, or of the subset
+    `indices` of them (a rank's shard); per-instance results keep the
+    instance's index in the full sweep."""
     insts = geometry.sweep_instances(seed, count)
+    index = list(range(count)) if indices is None else list(indices)
+    insts = [insts[k] for k in index]
+    count = len(insts)
     t0 = time.perf_counter()
     grids = [build_grid(i, storage) for i in insts]
     setup_s = time.perf_counter() - t0
@@ -87,7 +138,7 @@ def run_sweep(count: int = 64, steps: int = 3000, seed: int = 1, autotune: bool 
     }
     for k, (inst, g) in enumerate(zip(insts, grids)):
         res["per_instance"].append({
-            "index": k, "dims": list(inst["dims"]), "kind": inst["kind"], "op": inst["op"],
+            "index": index[k], "dims": list(inst["dims"]), "kind": inst["kind"], "op": inst["op"],
             "U": inst["U"], "Re": inst["Re"], "tau": float(g.s.tau),
             "tile": list(batch.tile(k)), "area": areas[k],
             "cd": drag_coefficient(g, inst["U"], areas[k]),
@@ -134,7 +185,27 @@ def main(argv=None) -> int:
     ap.add_argument("--no-solo", action="store_true")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
-    res = run_sweep(a.count, a.steps, a.seed, not a.no_autotune, not a.no_solo, a.storage)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    indices = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")) % torch.cuda.device_count())
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dims = [i["dims"] for i in geometry.sweep_instances(a.seed, a.count)]
+        indices = shard(dims, world, rank)
+    res = run_sweep(a.count, a.steps, a.seed, not a.no_autotune, not a.no_solo, a.storage,
+                    indices=indices)
+    if world > 1:
+        gathered = [None] * world
+        dist.all_gather_object(gathered, res)
+        dist.destroy_process_group()
+        if rank != 0:
+            return 0
+        res = merge_ranks(gathered)
     summary = {k: v for k, v in res.items() if k != "per_instance"}
     tiles = {}
     for p in res["per_instance"]:

@@ -82,3 +82,69 @@ def test_warmstart_entry_and_summaries():
     assert abs(s16["wall_ratio_total"] - 0.3 / 1.1) < 1e-12
     assert s16["steps_ratio_total"] == 3000 / 11000
     assert s16["faster_fraction"] == 1.0
+
+
+def test_sweep_shards_partition_and_balance():
+    from lattice_fluid_dynamics_b200 import sweep
+    dims = [i["dims"] for i in geometry.sweep_instances(1, 64)]
+    for world in (1, 2, 3, 4, 8):
+        parts = [sweep.shard(dims, world, r) for r in range(world)]
+        flat = sorted(k for p in parts for k in p)
+        assert flat == list(range(64))                      # every instance exactly once
+        loads = [sum(int(np.prod(dims[k])) for k in p) for p in parts]
+        assert max(loads) <= 1.05 * min(loads)              # near-equal lattice updates
+        assert parts == [sweep.shard(dims, world, r) for r in range(world)]  # deterministic
+
+
+def _fake_rank_result(rank, idx, ms):
+    return {"instances": len(idx), "steps": 100, "seed": 1, "storage": "fp32",
+            "cells_total": 1000 * len(idx), "ms": ms, "mlups": 0.0,
+            "gb_per_s": 10.0 * (rank + 1), "schedule": "graph", "cd_identical": len(idx),
+            "per_instance": [{"index": k, "cd": 0.1 * k} for k in idx]}
+
+
+def test_sweep_merge_ranks():
+    from lattice_fluid_dynamics_b200 import sweep
+    parts = [[0, 3], [1, 2, 4]]
+    res = sweep.merge_ranks([_fake_rank_result(r, p, 50.0 + 10 * r) for r, p in enumerate(parts)])
+    assert res["instances"] == 5 and res["ranks"] == 2 and res["ms"] == 60.0
+    assert [p["index"] for p in res["per_instance"]] == [0, 1, 2, 3, 4]
+    assert res["mlups"] == 5000 * 100 / 0.060 / 1e6
+    assert res["cd_identical"] == 5
+
+
+def _gather_rank(rank, world, port, out):
+    import os
+    import torch.distributed as dist
+    from lattice_fluid_dynamics_b200 import sweep
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        dims = [i["dims"] for i in geometry.sweep_instances(1, 64)]
+        mine = sweep.shard(dims, world, rank)
+        got = [None] * world
+        dist.all_gather_object(got, _fake_rank_result(rank, mine, 40.0 + rank))
+        if rank == 0:
+            res = sweep.merge_ranks(got)
+            out.put((res["instances"], [p["index"] for p in res["per_instance"]], res["ms"]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sweep_two_gloo_ranks_gather():
+    import socket
+
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_gather_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    n, order, ms = q.get(timeout=240)
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    assert n == 64 and order == list(range(64)) and ms == 41.0
