@@ -204,6 +204,50 @@ def cpu_oracle_run(budget_s: float, max_steps: int, warmup: int = 1):
     return NX * NY * NZ * steps / secs / 1e6, steps, secs, cores
 
 
+def cpu_table(budget_s: float) -> list:
+    """The oracle's FP32 BGK and MRT steps on the host cores at config 1
+    (128x64x64, sphere of radius 8 cells, tau 0.6, half-way bounce-back) and
+    config 2 (the bench workload, and the same with BGK): MLUPS from a
+    bounded number of steps after one untimed step."""
+    from lattice_fluid_dynamics_b200 import geometry as G
+    from oracle import pyoracle as po
+    po.build()
+    po.set_threads(0)
+    tris, bbox = G.ahmed_body()
+    c1 = ((32 + 0.5) / 16 - 4, (32 + 0.5) / 16 - 2, (32 + 0.5) / 16 - 2, 0.5)
+    cases = [
+        ("c1_sphere_128x64x64_bgk", (128, 64, 64), dict(), "sphere"),
+        ("c1_sphere_128x64x64_mrt", (128, 64, 64), dict(useMRT=1), "sphere"),
+        ("c2_ahmed_256x128x128_bgk", (NX, NY, NZ), dict(periodicYZ=1), "mesh"),
+        ("c2_ahmed_256x128x128_mrt_smagorinsky", (NX, NY, NZ), FLAGS, "mesh"),
+    ]
+    rows = []
+    for name, (nx, ny, nz), flags, body in cases:
+        if body == "sphere":
+            g = po.OracleGrid(nx, ny, nz, (0.6 - 0.5) / 3)
+            g.set(tau=0.6, **flags)
+            g.set_solid_sphere(*c1, halfway=True)
+        else:
+            g = po.OracleGrid(nx, ny, nz, 1e-4)
+            g.set(tau=tau_c2(), **flags)
+            g.set_solid_mesh(tris, bbox)
+        g.initialize_flow(U)
+        g.step(U)
+        t0 = time.perf_counter()
+        g.step(U)
+        per = time.perf_counter() - t0
+        n = max(1, int(budget_s / max(per, 1e-6)) - 1)
+        t0 = time.perf_counter()
+        g.step(U, n=n)
+        secs = time.perf_counter() - t0 + per
+        g.close()
+        rows.append({"case": name, "cells": nx * ny * nz, "steps": n + 1,
+                     "seconds": round(secs, 2),
+                     "mlups": round(nx * ny * nz * (n + 1) / secs / 1e6, 2),
+                     "threads": os.cpu_count() or 1, "kind": "port"})
+    return rows
+
+
 def reference_arm(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -241,11 +285,17 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--clocks-file", default=None)
+    ap.add_argument("--cpu-table", action="store_true",
+                    help="time the CPU oracle's BGK and MRT steps at configs 1 and 2, then exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
     if args.impl == "reference":
         return reference_arm(args)
+    if args.cpu_table:
+        for row in cpu_table(args.cpu_budget / 4):
+            print(json.dumps(row), flush=True)
+        return 0
 
     world, rank, phys, pg = dist_setup(args.gpus)
     import numpy as np
