@@ -395,20 +395,25 @@ __device__ __forceinline__ void mrt_forward(const R (&fi)[19], R (&m)[19]) {
 
 template <typename R>
 __device__ __forceinline__ void mrt_inverse(const R (&m)[19], R (&fi)[19]) {
+    // m_k / |M_k|^2 (lbm_collide.comp:187-205).  The divisors are constants
+    // checked with cdiv on all 2^32 inputs; a quotient that cdiv could get
+    // wrong has magnitude below 2^-93 and every population below sums it
+    // into terms led by m_0 / 19 = rho / 19, which absorb it either way.
+    auto q = [](R x, R y) { return cdiv<R>(x, y, R(1) / y); };
     R ms[19];
-    ms[0] = ddiv<R>(m[0], R(19));
-    ms[1] = ddiv<R>(m[1], R(2394));
-    ms[2] = ddiv<R>(m[2], R(252));
-    ms[3] = ddiv<R>(m[3], R(10));
-    ms[4] = ddiv<R>(m[4], R(40));
-    ms[5] = ddiv<R>(m[5], R(10));
-    ms[6] = ddiv<R>(m[6], R(40));
-    ms[7] = ddiv<R>(m[7], R(10));
-    ms[8] = ddiv<R>(m[8], R(40));
-    ms[9] = ddiv<R>(m[9], R(36));
-    ms[10] = ddiv<R>(m[10], R(72));
-    ms[11] = ddiv<R>(m[11], R(12));
-    ms[12] = ddiv<R>(m[12], R(24));
+    ms[0] = q(m[0], R(19));
+    ms[1] = q(m[1], R(2394));
+    ms[2] = q(m[2], R(252));
+    ms[3] = q(m[3], R(10));
+    ms[4] = q(m[4], R(40));
+    ms[5] = q(m[5], R(10));
+    ms[6] = q(m[6], R(40));
+    ms[7] = q(m[7], R(10));
+    ms[8] = q(m[8], R(40));
+    ms[9] = q(m[9], R(36));
+    ms[10] = q(m[10], R(72));
+    ms[11] = q(m[11], R(12));
+    ms[12] = q(m[12], R(24));
     ms[13] = m[13] * R(0.25);  // division by a power of two is exact
     ms[14] = m[14] * R(0.25);
     ms[15] = m[15] * R(0.25);
