@@ -8,6 +8,8 @@ Smagorinsky (Cs = 0.1), tau from Re = 5e4 at U = 0.05 set directly
 MB) are larger than the 126 MB L2, so consecutive steps stream from HBM.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+  python bench.py --op-table [--storage ...] [--op ...] [--arith ...] [--kernel ...]
+  python bench.py --cpu-table
 
 Under torchrun (N > 1) every rank runs an independent replica of the
 workload (the hot path is single-grid; multi-GPU is replicas only); value
@@ -273,6 +275,101 @@ def reference_arm(args):
 
 
 # ---------------------------------------------------------------------------
+# step-kernel table: every storage format, collision operator, arithmetic
+# mode and step kernel on the same Ahmed-body tunnel
+# ---------------------------------------------------------------------------
+TABLE_OPS = {
+    "bgk": dict(),
+    "reg": dict(useRegularized=1),
+    "mrt": dict(useMRT=1),
+    "mrt_smag": dict(useMRT=1, useSmagorinsky=1, smagorinskyCs=0.1),
+}
+
+
+def table_grid(dims, storage: str, op: str, arith: int, staged: bool, tris, bbox):
+    from lattice_fluid_dynamics_b200 import capi
+    nx, ny, nz = dims
+    g = capi.Grid(nx, ny, nz, 1e-4, storage=storage)
+    g.set(tau=tau_c2(), periodicYZ=1, arithmetic=arith, **TABLE_OPS[op])
+    if g.set_tma_staging(staged) != staged:
+        g.close()
+        raise RuntimeError(f"TMA staging unavailable for {storage} {dims}")
+    g.set_solid_mesh(tris, bbox)
+    g.initialize_flow(U)
+    return g
+
+
+def table_timed(g, steps: int) -> float:
+    """CUDA-event milliseconds of `steps` graph-replayed steps on the grid's
+    stream, after 64 untimed steps."""
+    import torch
+    g.step(U, n=64)
+    stream = torch.cuda.ExternalStream(g.stream_ptr())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    g.step(U, n=steps)
+    e1.record(stream)
+    e1.synchronize()
+    g.check()
+    return e0.elapsed_time(e1)
+
+
+def table_readbacks(g, k: int) -> dict:
+    """Host microseconds of one drag readback and of one LBM_Step + readback
+    (means over k; both are synchronous, so host time is the cost)."""
+    g.drag_force_decomposed()
+    t0 = time.perf_counter()
+    for _ in range(k):
+        g.drag_force_decomposed()
+    t1 = time.perf_counter()
+    for _ in range(k):
+        g.step(U)
+        g.drag_force_decomposed()
+    t2 = time.perf_counter()
+    g.check()
+    return {"readback_us": round(1e6 * (t1 - t0) / k, 1),
+            "step_readback_us": round(1e6 * (t2 - t1) / k, 1)}
+
+
+def op_table(args) -> int:
+    """One JSON line per (storage, operator, arithmetic, kernel): MLUPS and
+    GB/s of algorithmic population traffic over --table-steps graph-replayed
+    steps.  --loop N instead runs N single LBM_Step launches per case with no
+    timing (a short target for a profiler); --readback K adds K synchronous
+    drag readbacks per case (timed unless --loop)."""
+    from lattice_fluid_dynamics_b200 import geometry as G
+    dims = tuple(int(v) for v in args.dims.split("x"))
+    tris, bbox = G.ahmed_body()
+    cells = dims[0] * dims[1] * dims[2]
+    for storage in args.storage:
+        for op in args.op:
+            for arith in args.arith:
+                for kernel in args.kernel:
+                    g = table_grid(dims, storage, op, arith, kernel == "staged", tris, bbox)
+                    row = dict(storage=storage, op=op, arith=arith, kernel=kernel,
+                               dims=list(dims))
+                    if args.loop:
+                        g.step_loop(U, n=args.loop)
+                        for _ in range(args.readback):
+                            g.drag_force_decomposed()
+                        g.check()
+                    else:
+                        ms = table_timed(g, args.table_steps)
+                        sec = ms * 1e-3
+                        row.update(steps=args.table_steps, ms=round(ms, 3),
+                                   mlups=round(cells * args.table_steps / sec / 1e6, 1),
+                                   gb_per_s=round(cells * args.table_steps * g.bytes_per_update()
+                                                  / sec / 1e9, 1))
+                        if args.readback:
+                            row.update(table_readbacks(g, args.readback))
+                    g.close()
+                    print(json.dumps(row), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def main():
@@ -287,6 +384,21 @@ def main():
     ap.add_argument("--clocks-file", default=None)
     ap.add_argument("--cpu-table", action="store_true",
                     help="time the CPU oracle's BGK and MRT steps at configs 1 and 2, then exit")
+    ap.add_argument("--op-table", action="store_true",
+                    help="time the step kernel per storage / operator / arithmetic / kernel "
+                         "on the Ahmed-body tunnel, then exit")
+    ap.add_argument("--dims", default="256x128x128", help="--op-table grid")
+    ap.add_argument("--storage", nargs="+", default=["fp32", "fp16", "bf16"],
+                    help="--op-table storage formats")
+    ap.add_argument("--op", nargs="+", default=["bgk", "reg", "mrt_smag"],
+                    choices=sorted(TABLE_OPS), help="--op-table collision operators")
+    ap.add_argument("--arith", nargs="+", type=int, default=[0], choices=[0, 1],
+                    help="--op-table arithmetic: 0 exact, 1 fast")
+    ap.add_argument("--kernel", nargs="+", default=["direct"], choices=["direct", "staged"],
+                    help="--op-table step kernel: direct, or TMA-staged")
+    ap.add_argument("--table-steps", type=int, default=512, help="--op-table timed steps")
+    ap.add_argument("--loop", type=int, default=0, help="--op-table: untimed launches only")
+    ap.add_argument("--readback", type=int, default=0, help="--op-table: drag readbacks")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -296,6 +408,8 @@ def main():
         for row in cpu_table(args.cpu_budget / 4):
             print(json.dumps(row), flush=True)
         return 0
+    if args.op_table:
+        return op_table(args)
 
     world, rank, phys, pg = dist_setup(args.gpus)
     import numpy as np

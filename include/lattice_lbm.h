@@ -216,22 +216,29 @@ void LBM_StepN(LBMGrid *grid, int nSteps, float inletVelX, float inletVelY,
 int LBM_ComputeDragForceF64(LBMGrid *grid, double *out6, long long *raw7);
 
 /* Global sums in FP64 over all cells of the post-stream state:
- * out[0] = mass (sum of rho), out[1..3] = momentum. */
+ * out[0] = mass (sum of rho), out[1..3] = momentum.  Returns 1 on success,
+ * 0 on failure (as LBM_InitializeFlow). */
 int LBM_ComputeMassMomentum(LBMGrid *grid, double *out4);
 
 /* No counterpart in the reference.  FP64 mass and momentum (out4[0] =
  * sum of rho, out4[1..3] = momentum) of a caller-owned FP32 population field
- * in this library's SoA layout, populations[i * numCells + cell], on
- * `stream` (a cudaStream_t; NULL is the legacy default stream), written to
- * host memory out4 after the stream is synchronised.  It allocates nothing,
- * for callers that cannot call cudaMalloc (graph capture or replay, real-time
- * loops, memory owned by another allocator): the scratch is a fixed 128 KiB
- * __device__ array held per GPU for the life of the process, which limits
- * numCells to 268,435,456 (larger fields return LBM_ERR_INVALID_ARGUMENT).
- * The first call on each device looks up that array's device address
- * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
- * share the array: calls that overlap on the GPU race.  Returns LBM_OK or an
- * LBM_ERR_* code. */
+ * in this library's SoA layout, populations[i * numCells + cell], computed
+ * on `stream` (a cudaStream_t; NULL is the legacy default stream).  The call
+ * synchronises that stream and writes the four sums to host memory out4
+ * before it returns.  It allocates nothing, for callers that cannot call
+ * cudaMalloc: real-time loops that must not stall on an allocation, and
+ * applications whose device memory belongs to another allocator.  The
+ * scratch is a fixed 128 KiB __device__ array held per GPU for the life of
+ * the process, which limits numCells to 268,435,456.  The first call on each
+ * device looks up that array's device address (cudaGetSymbolAddress), so
+ * make it before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race.
+ * Return convention: LBM_OK (0) on success -- the opposite of
+ * LBM_ComputeMassMomentum, which returns 1 on success.  Errors:
+ * LBM_ERR_INVALID_ARGUMENT for a NULL pointer, numCells <= 0 or above the
+ * maximum (nothing is launched); LBM_ERR_CUDA when the address lookup, a
+ * launch or the copy fails, or when the stream synchronisation reports an
+ * error (which may come from earlier work on the same stream). */
 int LBM_MassMomentumNoAlloc(const float *populations, long long numCells,
                             double *out4, void *stream);
 

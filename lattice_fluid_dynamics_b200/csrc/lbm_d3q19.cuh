@@ -190,7 +190,7 @@ __device__ __forceinline__ double cdiv<double>(double x, double y, double) {
     return __ddiv_rn(x, y);
 }
 
-// Equilibrium (lbm_collide.comp:94-101, lbm_force.comp:216-221):
+// Equilibrium (lbm_collide.comp:94-101, lbm_force.comp:87-92):
 // feq_i(rho, u) = w_i rho (1 + eu/cs2 + eu^2/(2 cs2^2) - u^2/(2 cs2))
 // evaluated in the reference's order (lbm.c:37-44).  The three quotients
 // are by the constants cs2, 2 cs2^2 and 2 cs2 and use cdiv, which equals

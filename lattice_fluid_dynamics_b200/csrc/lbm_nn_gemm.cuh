@@ -18,8 +18,11 @@
 // Each 64-wide slice of the reduction is gathered by all threads into one of
 // two shared-memory stages, then one thread issues four K = 16 MMAs and
 // commits them to the stage's mbarrier; a stage is refilled only after its
-// previous MMAs completed.  Every wait is bounded: a wait that gives up sets
-// *err and the kernel still frees its tensor memory and returns.
+// previous MMAs completed.  Every wait is bounded.  When a wait gives up the
+// whole CTA stops: no stage is written and no MMA issued after it, the MMAs
+// already committed are drained (a bounded wait on the last commit), the
+// epilogue is skipped, *err gets bit 0 (bit 1 as well if the drain ran out),
+// and the tensor memory is freed before the kernel returns.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -119,11 +122,21 @@ __device__ __forceinline__ void gemm_tile(int nchunks, int *err, Load load, Epi 
     tc::fence_after_sync();
     const uint32_t tmem = *tslot;
     constexpr uint32_t idesc = tc::idesc_bf16_f32(128, NT);
-    bool ok = true;
+    bool ok = true;   // block-uniform: every wait so far completed
+    int issued = 0;   // chunks whose MMAs were issued and committed
 
     for (int c = 0; c < nchunks; c++) {
         const int s = c & 1;
-        if (c >= 2 && !tc::mbar_wait(bar[s], ((c >> 1) - 1) & 1, WAIT_LIMIT)) ok = false;
+        if (c >= 2) {
+            // stage s is refilled only once the MMAs of chunk c - 2 have read
+            // it; the vote makes the decision block-uniform, so after a wait
+            // that gave up no thread writes the stage and no MMA is issued
+            const bool got = tc::mbar_wait(bar[s], ((c >> 1) - 1) & 1, WAIT_LIMIT);
+            if (!__syncthreads_and(got)) {
+                ok = false;
+                break;
+            }
+        }
         load(c, a_st[s], b_st[s]);
         tc::fence_async_smem();
         __syncthreads();
@@ -138,30 +151,46 @@ __device__ __forceinline__ void gemm_tile(int nchunks, int *err, Load load, Epi 
             }
             tc::mma_commit(bar[s]);
         }
+        issued = c + 1;
     }
-    if (nchunks > 0) {
-        const int c = nchunks - 1;
-        if (!tc::mbar_wait(bar[c & 1], (c >> 1) & 1, WAIT_LIMIT)) {
+    // Drain: the commit of the last issued chunk completes only when every
+    // MMA issued before it has completed, so once it has arrived nothing
+    // writes the accumulator or reads a stage any more.  The tensor core
+    // always finishes its MMAs, so this wait depends on nothing outside the
+    // CTA; it is still bounded (two limits).
+    bool drained = true;
+    if (issued > 0) {
+        const int c = issued - 1;
+        bool got = tc::mbar_wait(bar[c & 1], (c >> 1) & 1, WAIT_LIMIT);
+        if (!__syncthreads_and(got)) {
             ok = false;
-            tc::mbar_wait(bar[c & 1], (c >> 1) & 1, WAIT_LIMIT);  // second, final chance
+            got = tc::mbar_wait(bar[c & 1], (c >> 1) & 1, WAIT_LIMIT);
+            drained = __syncthreads_and(got) != 0;
         }
     }
     tc::fence_after_sync();
-    if (!ok) atomicExch(err, 1);
-    const int row = warp * 32 + (tid & 31);
+    if (!ok && tid == 0) atomicOr(err, drained ? 1 : 3);
+    if (ok) {
+        // the accumulator is complete: read it back and hand it to the epilogue
+        const int row = warp * 32 + (tid & 31);
 #pragma unroll 1
-    for (int col = 0; col < NT; col += 8) {
-        float v[8];
-        tc::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)col, v);
-        tc::tmem_wait_ld();
-        if (nchunks == 0) {
+        for (int col = 0; col < NT; col += 8) {
+            float v[8];
+            tc::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)col, v);
+            tc::tmem_wait_ld();
+            if (nchunks == 0) {
 #pragma unroll
-            for (int i = 0; i < 8; i++) v[i] = 0.f;
+                for (int i = 0; i < 8; i++) v[i] = 0.f;
+            }
+            epi(row, col, v);
         }
-        epi(row, col, v);
     }
     tc::fence_before_sync();
     __syncthreads();
+    // Freed in every case: a CTA that exits holding tensor memory would leave
+    // later CTAs on its SM blocked in tcgen05.alloc.  If the drain itself ran
+    // out (error bit 1 set beside bit 0) an MMA might still be writing those
+    // columns; the launch's results are discarded through the error word.
     if (warp == 0) tc::tmem_dealloc(tmem, ncols);
 }
 

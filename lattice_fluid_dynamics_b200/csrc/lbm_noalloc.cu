@@ -3,13 +3,15 @@
 //
 // This is the allocation-free variant of the FP64 reduction behind
 // LBM_ComputeMassMomentum (k_mass_momentum, which accumulates into scratch
-// that LBM_Create allocates).  Some callers cannot call cudaMalloc: code
-// that runs while a CUDA graph is being captured or replayed, real-time
-// loops that must not synchronise the device the way an allocation can,
-// and hosts whose memory is owned by another allocator or framework.  They
-// keep their populations in their own device buffer and need the mass and
-// momentum of it.  Here the scratch is a file-scope __device__ array of a
-// fixed size, so nothing is allocated at call time.
+// that LBM_Create allocates).  Some callers cannot call cudaMalloc: real-time
+// loops that must not stall on an allocation (cudaMalloc may synchronise the
+// device and its cost is unbounded), and host applications whose device
+// memory is owned and budgeted by another allocator or framework, so that a
+// library may not take any of it for itself.  They keep their populations in
+// their own device buffer and need the mass and momentum of it.  Here the
+// scratch is a file-scope __device__ array of a fixed size, so nothing is
+// allocated at call time.  The call synchronises the caller's stream and
+// copies the four sums to host memory before it returns.
 //
 // Scratch: one FP64 partial (mass, jx, jy, jz) per chunk of 65,536 cells,
 // at most 4,096 chunks, plus the four totals: 4,096 * 4 * 8 + 32 bytes
@@ -114,10 +116,16 @@ extern "C" int LBM_MassMomentumNoAlloc(const float *populations, long long numCe
     double *scratch = nullptr;
     if (scratch_on_current_device(&scratch) != cudaSuccess) return LBM_ERR_CUDA;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int nchunks = (int)((numCells + kChunkCells - 1) / kChunkCells);
-    k_partials<<<nchunks, kThreads, 0, s>>>(populations, numCells, scratch);
-    k_totals<<<1, 32, 0, s>>>(nchunks, scratch);
-    if (cudaGetLastError() != cudaSuccess) return LBM_ERR_CUDA;
+    int nchunks = (int)((numCells + kChunkCells - 1) / kChunkCells);
+    // launched through cudaLaunchKernel so that the status checked is this
+    // call's own, not an error left behind by earlier unrelated work
+    void *pargs[] = {&populations, &numCells, &scratch};
+    if (cudaLaunchKernel((const void *)k_partials, dim3(nchunks), dim3(kThreads), pargs, 0, s) !=
+        cudaSuccess)
+        return LBM_ERR_CUDA;
+    void *targs[] = {&nchunks, &scratch};
+    if (cudaLaunchKernel((const void *)k_totals, dim3(1), dim3(32), targs, 0, s) != cudaSuccess)
+        return LBM_ERR_CUDA;
     if (cudaMemcpyAsync(out4, scratch + 4 * kMaxChunks, 4 * sizeof(double),
                         cudaMemcpyDeviceToHost, s) != cudaSuccess)
         return LBM_ERR_CUDA;

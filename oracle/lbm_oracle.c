@@ -501,6 +501,22 @@ void or_mrt_meq_f32(float rho, float ux, float uy, float uz, float *meq) {
 }
 float or_weight_f32(int i) { return wgt_f32(i); }
 
+/* Batched forms of the above for the comparisons against the reference's own
+ * C mirrors (simulation/test/test_lbm.c:71-187) on millions of states:
+ * out[19 k + i] = feq(i, state[4 k .. 4 k + 3]) with state = (rho, ux, uy, uz). */
+void or_feq_batch_f32(int64_t n, const float *state, float *out) {
+    for (int64_t k = 0; k < n; k++) {
+        const float *s = state + 4 * k;
+        for (int i = 0; i < 19; i++) out[19 * k + i] = feq_f32(i, s[0], s[1], s[2], s[3]);
+    }
+}
+void or_mrt_forward_batch_f32(int64_t n, const float *fi, float *m) {
+    for (int64_t k = 0; k < n; k++) mrt_fwd_f32(fi + 19 * k, m + 19 * k);
+}
+void or_mrt_inverse_batch_f32(int64_t n, const float *m, float *fi) {
+    for (int64_t k = 0; k < n; k++) mrt_inv_f32(m + 19 * k, fi + 19 * k);
+}
+
 /* ---- particles ---- */
 
 /* 32-bit counter hash (three rounds of the "lowbias32" integer mixer of

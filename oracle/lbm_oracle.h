@@ -21,8 +21,11 @@
  *
  * Parity pins: the known-answer tests of simulation/test/test_lbm.c:191-366
  * (weights, equilibrium moments, MRT transforms) run against this code in
- * tests/test_oracle_kat.py, and tests/golden/ holds the fixtures generated
- * from it together with the script that made them.
+ * tests/test_oracle_kat.py; feq and the two MRT transforms are required to
+ * equal, bit for bit, the reference's own CPU mirrors of them
+ * (test_lbm.c:43-187, compiled by `make -C oracle ref`) in
+ * tests/test_ref_math_cpu.py, against the fixture tests/golden/
+ * ref_math.json that tests/golden/make_ref_math.py made from them.
  */
 #ifndef LBM_ORACLE_H
 #define LBM_ORACLE_H
@@ -96,6 +99,10 @@ void or_mrt_forward_f32(const float *fi, float *m);
 void or_mrt_inverse_f32(const float *m, float *fi);
 void or_mrt_meq_f32(float rho, float ux, float uy, float uz, float *meq);
 float or_weight_f32(int i);
+/* batched over n states (state = rho, ux, uy, uz; 19 values per state out) */
+void or_feq_batch_f32(int64_t n, const float *state, float *out);
+void or_mrt_forward_batch_f32(int64_t n, const float *fi, float *m);
+void or_mrt_inverse_batch_f32(int64_t n, const float *m, float *fi);
 
 /* ---- particles (particle_lbm.comp:46-89 sampler, :207-293 Euler step,
  * collisionMode 0).  Particle = 8 floats {x,y,z,pad,vx,vy,vz,life}.  The

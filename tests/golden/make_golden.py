@@ -1,7 +1,7 @@
 """Generate the golden fixtures for OBJ ingestion and Strouhal extraction.
 
 The expected outputs come from the reference's own C sources, compiled by
-``make -C oracle ref`` into ``oracle/_ref/libref_host.so`` from
+``make -C oracle ref REFSIM=<reference>/simulation`` into ``oracle/_ref/libref_host.so`` from
 simulation/obj-file-loader/lib/model_loader.c, simulation/src/model_bounds.c
 and simulation/src/drag_metrics.c (only possible where the reference tree is
 present).  The inputs are synthetic: small OBJ files written below that
@@ -50,7 +50,7 @@ class RefBounds(C.Structure):
 
 def load_ref():
     if not os.path.exists(REF_LIB):
-        sys.exit(f"{REF_LIB} missing: run `make -C oracle ref` where the reference tree exists")
+        sys.exit(f"{REF_LIB} missing: run `make -C oracle ref REFSIM=<reference>/simulation` where the reference tree exists")
     lib = C.CDLL(REF_LIB)
     lib.loadOBJ.restype = RefModel
     lib.loadOBJ.argtypes = [C.c_char_p]

@@ -7,6 +7,13 @@
 // operations on edge inputs.
 //
 // usage: collide_check <out.bin> <n_states>
+//        collide_check --math <state.bin> <fi.bin> <m.bin> <n> <out.bin>
+// The second form evaluates, for n given states, the device's equilibrium
+// (feq one direction at a time, and the step's equilibria() of all 19), MRT
+// forward transform and MRT inverse transform, and writes them as float32
+// [4][n][19]; tests/test_collide_native_gpu.py compares them with the
+// reference's own C mirrors of that arithmetic (simulation/test/
+// test_lbm.c:43-187) through tests/golden/ref_math.json.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -81,7 +88,63 @@ __global__ void k_pairs(int n, unsigned *bad) {
         atomicAdd(bad + 4, 1u);
 }
 
+__global__ void k_math(int n, const float *state, const float *fi, const float *mi, float *out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float rho = state[4 * k], ux = state[4 * k + 1], uy = state[4 * k + 2],
+                uz = state[4 * k + 3];
+    float a[19], b[19];
+    const long long o = (long long)k * 19, plane = (long long)n * 19;
+    for (int i = 0; i < 19; i++) out[o + i] = feq<float>(i, rho, ux, uy, uz);
+    equilibria<float>(rho, ux, uy, uz, a);
+    for (int i = 0; i < 19; i++) out[plane + o + i] = a[i];
+    for (int i = 0; i < 19; i++) a[i] = fi[o + i];
+    mrt_forward<float>(a, b);
+    for (int i = 0; i < 19; i++) out[2 * plane + o + i] = b[i];
+    for (int i = 0; i < 19; i++) a[i] = mi[o + i];
+    mrt_inverse<float>(a, b);
+    for (int i = 0; i < 19; i++) out[3 * plane + o + i] = b[i];
+}
+
+static bool read_file(const char *path, std::vector<float> &v) {
+    FILE *f = fopen(path, "rb");
+    if (!f) return false;
+    const size_t got = fread(v.data(), sizeof(float), v.size(), f);
+    fclose(f);
+    return got == v.size();
+}
+
+static int math_mode(int argc, char **argv) {
+    if (argc < 7) return 2;
+    const int n = atoi(argv[5]);
+    if (n <= 0) return 2;
+    std::vector<float> st((size_t)4 * n), fi((size_t)19 * n), mi((size_t)19 * n);
+    if (!read_file(argv[2], st) || !read_file(argv[3], fi) || !read_file(argv[4], mi)) return 8;
+    float *d_st = nullptr, *d_fi = nullptr, *d_mi = nullptr, *d_out = nullptr;
+    if (cudaMalloc(&d_st, st.size() * 4) != cudaSuccess ||
+        cudaMalloc(&d_fi, fi.size() * 4) != cudaSuccess ||
+        cudaMalloc(&d_mi, mi.size() * 4) != cudaSuccess ||
+        cudaMalloc(&d_out, (size_t)4 * 19 * n * 4) != cudaSuccess)
+        return 3;
+    cudaMemcpy(d_st, st.data(), st.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_fi, fi.data(), fi.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_mi, mi.data(), mi.size() * 4, cudaMemcpyHostToDevice);
+    k_math<<<(n + 127) / 128, 128>>>(n, d_st, d_fi, d_mi, d_out);
+    std::vector<float> h((size_t)4 * 19 * n);
+    if (cudaMemcpy(h.data(), d_out, h.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return 4;
+    FILE *fo = fopen(argv[6], "wb");
+    if (!fo) return 5;
+    fwrite(h.data(), sizeof(float), h.size(), fo);
+    fclose(fo);
+    cudaFree(d_st);
+    cudaFree(d_fi);
+    cudaFree(d_mi);
+    cudaFree(d_out);
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 6;
+}
+
 int main(int argc, char **argv) {
+    if (argc >= 2 && strcmp(argv[1], "--math") == 0) return math_mode(argc, argv);
     if (argc < 3) return 2;
     const int n = atoi(argv[2]);
     float *d = nullptr;

@@ -4,7 +4,7 @@ The fixtures in tests/golden/host_golden.json were produced by the
 reference's loadOBJ, computeModelBounds, createTriangleBuffer
 (simulation/obj-file-loader/lib/model_loader.c, simulation/src/model_bounds.c)
 and compute_strouhal (simulation/src/drag_metrics.c), compiled from their
-sources by ``make -C oracle ref``; tests/golden/make_golden.py regenerates
+sources by ``make -C oracle ref REFSIM=<reference>/simulation``; tests/golden/make_golden.py regenerates
 them.  Comparisons are bit-exact (float bytes, printed strings).  When
 oracle/_ref/libref_host.so is present the live reference is also run on
 freshly generated meshes.
