@@ -40,8 +40,8 @@ def _headers_mtime():
     return max(os.path.getmtime(h) for h in hs)
 
 
-# the fast-arithmetic translation units (lbm_step_fast.cu) contract FMAs and
-# use approximate division / square root
+# the fast-arithmetic translation units (lbm_step_fast_*.cu) contract FMAs
+# and use approximate division / square root
 FAST_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=true", "-prec-div=false",
               "-prec-sqrt=false", "-ftz=false", "-Xcompiler", "-fPIC,-ffp-contract=off",
               "-I" + os.path.join(HERE, "..", "include")]
@@ -52,7 +52,7 @@ def _compile(src: str, verbose_ptxas: bool) -> str:
     if (os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src)
             and os.path.getmtime(obj) >= _headers_mtime()):
         return obj
-    flags = FAST_FLAGS if src.endswith("_fast.cu") else FLAGS
+    flags = FAST_FLAGS if os.path.basename(src).startswith("lbm_step_fast") else FLAGS
     cmd = [NVCC, *ARCH, *flags, "-c", src, "-o", obj]
     if verbose_ptxas:
         cmd += ["-Xptxas", "-v"]

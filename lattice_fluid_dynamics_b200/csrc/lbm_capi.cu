@@ -54,15 +54,18 @@ size_t elem_size(int storage) {
     }
 }
 
-// Step launch shape: 256-thread blocks of 32 x 8 cells (a warp spans 32
-// consecutive x), at least 4 blocks resident per SM (<= 64 registers).
-// Measured on B200 at 256x128x128 against 64x4 / 128x2 / 256x1 shapes and
-// an unconstrained register budget.  LBM_BLOCK=<bx>x<by>, LBM_MINB=1|4 and
-// LBM_CPT=1|2 override it.
+// Step launch shape.  FP32 / FP16 / BF16 grids with an even NX run the
+// paired kernel (two cells per thread, cpt = 2; 128-thread blocks of 32 x 4
+// threads, 64 x 4 cells).  Otherwise (FP64, odd NX, or LBM_CPT=1): 256-thread
+// blocks of 32 x 8 cells (a warp spans 32 consecutive x), at least 4 blocks
+// resident per SM (<= 64 registers), measured on B200 at 256x128x128 against
+// 64x4 / 128x2 / 256x1 shapes and an unconstrained register budget.
+// LBM_BLOCK=<bx>x<by>, LBM_MINB=1|4 and LBM_CPT=1|2 override it.
 void default_block(GridImpl &I) {
     I.bx = 32;
     I.by = 8;
     I.cpt = 1;
+    I.pbx = 32;
     I.minb = 4;
     const char *cenv = getenv("LBM_CPT");
     if (cenv) I.cpt = atoi(cenv) == 2 ? 2 : 1;

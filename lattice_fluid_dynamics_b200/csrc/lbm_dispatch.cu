@@ -1,44 +1,56 @@
-// Storage-format dispatch of the step kernels (instantiated in
-// lbm_step_{f32,f64,f16,bf16}.cu).
+// Storage-format dispatch of the step kernels.  The kernels are
+// instantiated in lbm_step_{f32,f64,f16,bf16}.cu and lbm_step_fast_*.cu,
+// each of which exports a StepOps table; this unit sees only the tables.
 #include <cudaTypedefs.h>
 #include <stdlib.h>
 
-#include "lbm_step.cuh"
+#include "lbm_internal.h"
 
 namespace lbm {
 
-using namespace exact;
-extern template struct exact::StepLaunch<exact::StoreF32>;
-extern template struct exact::StepLaunch<exact::StoreF64>;
-extern template struct exact::StepLaunch<exact::StoreF16>;
-extern template struct exact::StepLaunch<exact::StoreBF16>;
-
-#define LBM_DISPATCH_INTO(out, storage, CALL)                        \
-    switch (storage) {                                                \
-        case LBM_STORAGE_FP32: out = StepLaunch<StoreF32>::CALL; break; \
-        case LBM_STORAGE_FP16: out = StepLaunch<StoreF16>::CALL; break; \
-        case LBM_STORAGE_BF16: out = StepLaunch<StoreBF16>::CALL; break; \
-        default: out = cudaErrorNotSupported; break;                  \
+static const StepOps *ops_of(int storage) {
+    switch (storage) {
+        case LBM_STORAGE_FP32: return &step_ops_f32;
+        case LBM_STORAGE_FP64: return &step_ops_f64;
+        case LBM_STORAGE_FP16: return &step_ops_f16;
+        case LBM_STORAGE_BF16: return &step_ops_bf16;
+        default: return nullptr;
     }
+}
 
-#define LBM_DISPATCH(storage, CALL)                               \
-    switch (storage) {                                            \
-        case LBM_STORAGE_FP32: return StepLaunch<StoreF32>::CALL; \
-        case LBM_STORAGE_FP64: return StepLaunch<StoreF64>::CALL; \
-        case LBM_STORAGE_FP16: return StepLaunch<StoreF16>::CALL; \
-        case LBM_STORAGE_BF16: return StepLaunch<StoreBF16>::CALL; \
-        default: return cudaErrorInvalidValue;                    \
+static const StepOps *fast_ops_of(int storage) {
+    switch (storage) {
+        case LBM_STORAGE_FP32: return &step_ops_fast_f32;
+        case LBM_STORAGE_FP16: return &step_ops_fast_f16;
+        case LBM_STORAGE_BF16: return &step_ops_fast_bf16;
+        default: return nullptr;
     }
+}
+
+#define LBM_DISPATCH(storage, CALL)                   \
+    do {                                              \
+        const StepOps *ops_ = ops_of(storage);        \
+        if (!ops_) return cudaErrorInvalidValue;      \
+        return ops_->CALL;                            \
+    } while (0)
 
 cudaError_t launch_step(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
                         bool fast_arith, cudaStream_t s) {
-    if (fast_arith && g.storage != LBM_STORAGE_FP64)
-        return fast::launch_step_fast(g, a, fused, op, smag, s);
+    if (fast_arith && g.storage != LBM_STORAGE_FP64) {
+        const StepOps *f = fast_ops_of(g.storage);
+        if (!f) return cudaErrorInvalidValue;
+        return f->step(g, a, fused, op, smag, s);
+    }
     LBM_DISPATCH(g.storage, step(g, a, fused, op, smag, s));
 }
 
 cudaError_t launch_step_batch(int storage, const BatchLaunchParams &p, int set, cudaStream_t s) {
     LBM_DISPATCH(storage, batch(p, set, s));
+}
+
+cudaError_t launch_step_batch_pair(int storage, const BatchPairParams &p, int set,
+                                   cudaStream_t s) {
+    LBM_DISPATCH(storage, batch_pair(p, set, s));
 }
 
 // the driver's tensor-map encoder, looked up once through the runtime
@@ -86,9 +98,9 @@ void setup_tma(GridImpl &g, bool force) {
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return;
     }
-    cudaError_t e = cudaSuccess;
-    LBM_DISPATCH_INTO(e, g.storage, tma_prepare());
-    if (e == cudaSuccess) e = fast::tma_prepare_fast(g.storage);
+    const StepOps *ops = ops_of(g.storage), *fops = fast_ops_of(g.storage);
+    cudaError_t e = (ops && fops) ? ops->tma_prepare() : cudaErrorNotSupported;
+    if (e == cudaSuccess) e = fops->tma_prepare();
     if (e != cudaSuccess) {
         cudaGetLastError();
         return;

@@ -76,8 +76,10 @@ struct GridImpl {
     float vin_inlet[3] = {0, 0, 0};
 
     // launch configuration of the step kernel: block shape and cells per
-    // thread along x
+    // thread along x (cpt = 2: the paired kernel, with pbx threads along x
+    // and 128 / pbx rows per block)
     int bx = 128, by = 1, cpt = 1, minb = 1;
+    int pbx = 32;
 
     // CUDA graphs for LBM_StepN, one per starting buffer parity (gbuf)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -132,6 +134,28 @@ struct StepOffsets {
     long long dir[19];
 };
 
+// Kernel parameter of the paired (two cells per thread) step: per-direction
+// base pointers so that every access is a 32-bit cell index added to a
+// parameter.
+struct PairTable {
+    const void *pull[19];  // src + i*n - (e_x + e_y NX + e_z NX NY): pulled value of an interior cell
+    const void *own[19];   // src + i*n: the cell's own value in plane i
+    void *dst[19];         // dst + i*n
+    float2 nz;             // (-0, -0): addend of the paired products
+};
+
+// One grid of a batched paired step launch (k_step_batch_pair), kept in
+// device memory (one table per buffer parity) and copied into shared memory
+// by each block that works on the grid.
+struct alignas(16) BatchGridDev {
+    StepArgs a;
+    PairTable t;
+    int combo;    // op * 2 + smagorinsky
+    int lbx;      // 1 << lbx threads along x (two cells each), 128 >> lbx rows
+    int tiles_x;
+    int tiles_y;
+};
+
 // One grid of a batched step launch (k_step_batch): its step arguments,
 // operator, and tile shape -- 1 << lbx cells along x (32..256) by
 // 256 >> lbx rows, tiles_x * tiles_y tiles per z plane.
@@ -179,13 +203,44 @@ struct BatchLaunchParams {
     int count;
 };
 cudaError_t launch_step_batch(int storage, const BatchLaunchParams &p, int set, cudaStream_t s);
+
+// Arguments of one batched paired launch: the grids' entries in device
+// memory, and work unit t (one tile of one z-plane) belonging to grid g with
+// starts[g] <= t < starts[g + 1].
+struct BatchPairParams {
+    const BatchGridDev *grids;
+    unsigned starts[BATCH_LAUNCH_MAX + 1];
+    int count;
+};
+cudaError_t launch_step_batch_pair(int storage, const BatchPairParams &p, int set,
+                                   cudaStream_t s);
+
+// The launchers of one storage format and arithmetic flavour.  Each step
+// translation unit (lbm_step_{f32,f16,bf16,f64}.cu, lbm_step_fast_*.cu)
+// instantiates the kernels of its format and exports one table; the
+// dispatcher (lbm_dispatch.cu) sees only these tables, so no kernel is
+// compiled twice.
+struct StepOps {
+    cudaError_t (*step)(const GridImpl &, const StepArgs &, bool fused, int op, bool smag,
+                        cudaStream_t);
+    cudaError_t (*batch)(const BatchLaunchParams &, int set, cudaStream_t);
+    cudaError_t (*batch_pair)(const BatchPairParams &, int set, cudaStream_t);
+    cudaError_t (*tma_prepare)();
+    cudaError_t (*stream_only)(const GridImpl &, const StepArgs &, cudaStream_t);
+    cudaError_t (*velocity)(const GridImpl &, const StepArgs &, int kind, float4 *, double4 *,
+                            cudaStream_t);
+    cudaError_t (*init_uniform)(const GridImpl &, void *, void *, float, float, float,
+                                cudaStream_t);
+    cudaError_t (*init_field)(const GridImpl &, void *, void *, const float *, const float *,
+                              cudaStream_t);
+    cudaError_t (*export_aos)(const GridImpl &, const void *, void *, bool, cudaStream_t);
+    cudaError_t (*import_aos)(const GridImpl &, const float *, void *, cudaStream_t);
+    cudaError_t (*mass_momentum)(const GridImpl &, const void *, double *, cudaStream_t);
+};
+extern const StepOps step_ops_f32, step_ops_f16, step_ops_bf16, step_ops_f64;
+extern const StepOps step_ops_fast_f32, step_ops_fast_f16, step_ops_fast_bf16;
 cudaError_t launch_step(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
                         bool fast_arith, cudaStream_t s);
-namespace fast {
-cudaError_t launch_step_fast(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
-                             cudaStream_t s);
-cudaError_t tma_prepare_fast(int storage);
-}
 // Encode the grid's TMA descriptors and allow k_step_tma's shared memory;
 // sets g.tma (false for FP64 storage or rows that are not a multiple of 16
 // bytes, and, unless `force`, unless LBM_TMA=1 is set in the environment).

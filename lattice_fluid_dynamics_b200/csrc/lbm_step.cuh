@@ -577,6 +577,15 @@ __global__ void __launch_bounds__(256) k_mass_momentum(const typename S::T *__re
     }
 }
 
+}  // namespace LBM_ARITH_NS
+}  // namespace lbm
+
+// the two-cells-per-thread paired step (uses the per-cell pieces above)
+#include "lbm_step_pair.cuh"
+
+namespace lbm {
+namespace LBM_ARITH_NS {
+
 // ---------------------------------------------------------------------
 // Host-side launchers for one storage format
 // ---------------------------------------------------------------------
@@ -590,13 +599,12 @@ struct StepLaunch {
     // whether a fused step of this grid runs k_step_tma
     static bool use_tma(const GridImpl &g, const StepArgs &a) {
         return sizeof(typename S::T) <= 4 && g.tma && g.bx == 32 && g.by == TMA_BOX_Y &&
-               g.cpt == 1 && (a.src == g.pop[0] || a.src == g.pop[1]);
+               (a.src == g.pop[0] || a.src == g.pop[1]);
     }
 
     template <int OP, bool SMAG>
     static void go(const GridImpl &g, const StepArgs &a, bool fused, cudaStream_t s) {
         const dim3 blk(g.bx, g.by, 1);
-        const int cpt = (g.cpt == 2 && g.nx % 2 == 0) ? 2 : 1;
         if constexpr (sizeof(typename S::T) <= 4) {
             if (fused && use_tma(g, a)) {
                 const dim3 grd((g.nx + 31) / 32, (g.ny + TMA_BOX_Y - 1) / TMA_BOX_Y,
@@ -607,6 +615,19 @@ struct StepLaunch {
                 return;
             }
         }
+        if constexpr (sizeof(typename S::T) <= 4) {
+            if (use_pair(g)) {
+                const PairTable t = pair_table(a);
+                const int pbx = g.pbx, pby = PAIR_THREADS / g.pbx;
+                const dim3 grd((g.nx / 2 + pbx - 1) / pbx, (g.ny + pby - 1) / pby, g.nz);
+                const dim3 blk2(pbx, pby, 1);
+                if (fused)
+                    k_step_pair<S, OP, SMAG, true><<<grd, blk2, 0, s>>>(a, t);
+                else
+                    k_step_pair<S, OP, SMAG, false><<<grd, blk2, 0, s>>>(a, t);
+                return;
+            }
+        }
         StepOffsets o;
         const long long plane = (long long)a.nx * a.ny;
         for (int i = 0; i < 19; i++) {
@@ -614,15 +635,35 @@ struct StepLaunch {
             o.pull[i] = o.dir[i] - cx(i) - cy(i) * (long long)a.nx - cz(i) * plane;
         }
         if (fused) {
-            if (cpt == 2)
-                k_step<S, OP, SMAG, true, 2, 1><<<grid3(g, 2), blk, 0, s>>>(a, o);
-            else if (g.minb == 4)
+            if (g.minb == 4)
                 k_step<S, OP, SMAG, true, 1, 4><<<grid3(g, 1), blk, 0, s>>>(a, o);
             else
                 k_step<S, OP, SMAG, true, 1, 1><<<grid3(g, 1), blk, 0, s>>>(a, o);
         } else {
             k_step<S, OP, SMAG, false, 1, 1><<<grid3(g, 1), blk, 0, s>>>(a, o);
         }
+    }
+
+    // whether a step of this grid runs the two-cells-per-thread paired kernel:
+    // FP32 / FP16 / BF16 storage, an even NX and cell indices below 2^31
+    static bool use_pair(const GridImpl &g) {
+        return sizeof(typename S::T) <= 4 && g.cpt == 2 && g.nx % 2 == 0 &&
+               g.n < (1ll << 31) && (g.pbx == 32 || g.pbx == 64 || g.pbx == 128);
+    }
+
+    static PairTable pair_table(const StepArgs &a) {
+        using T = typename S::T;
+        PairTable t;
+        const T *src = static_cast<const T *>(a.src);
+        T *dst = static_cast<T *>(a.dst);
+        const long long plane = (long long)a.nx * a.ny;
+        for (int i = 0; i < 19; i++) {
+            t.own[i] = src + (long long)i * a.n;
+            t.pull[i] = src + (long long)i * a.n - cx(i) - cy(i) * (long long)a.nx - cz(i) * plane;
+            t.dst[i] = dst + (long long)i * a.n;
+        }
+        t.nz = make_float2(-0.0f, -0.0f);
+        return t;
     }
 
     static cudaError_t step(const GridImpl &g, const StepArgs &a, bool fused, int op, bool smag,
@@ -712,6 +753,31 @@ struct StepLaunch {
         return cudaGetLastError();
     }
 
+    static cudaError_t batch_pair(const BatchPairParams &p, int set, cudaStream_t s) {
+        if constexpr (sizeof(typename S::T) <= 4) {
+            const unsigned tiles = p.starts[p.count];
+            if (p.count <= 0 || p.count > BATCH_LAUNCH_MAX || tiles == 0 || !p.grids)
+                return cudaErrorInvalidValue;
+            const dim3 blk(PAIR_THREADS);
+            switch (set) {
+                case BATCH_SET_BGK: k_step_batch_pair<S, BATCH_SET_BGK><<<tiles, blk, 0, s>>>(p); break;
+                case BATCH_SET_BGK_SMAG: k_step_batch_pair<S, BATCH_SET_BGK_SMAG><<<tiles, blk, 0, s>>>(p); break;
+                case BATCH_SET_REG: k_step_batch_pair<S, BATCH_SET_REG><<<tiles, blk, 0, s>>>(p); break;
+                case BATCH_SET_REG_SMAG: k_step_batch_pair<S, BATCH_SET_REG_SMAG><<<tiles, blk, 0, s>>>(p); break;
+                case BATCH_SET_MRT: k_step_batch_pair<S, BATCH_SET_MRT><<<tiles, blk, 0, s>>>(p); break;
+                case BATCH_SET_MRT_SMAG: k_step_batch_pair<S, BATCH_SET_MRT_SMAG><<<tiles, blk, 0, s>>>(p); break;
+                case BATCH_SET_BGK_REG: k_step_batch_pair<S, BATCH_SET_BGK_REG><<<tiles, blk, 0, s>>>(p); break;
+                default: k_step_batch_pair<S, BATCH_SET_ALL><<<tiles, blk, 0, s>>>(p); break;
+            }
+            return cudaGetLastError();
+        } else {
+            (void)p;
+            (void)set;
+            (void)s;
+            return cudaErrorNotSupported;
+        }
+    }
+
     static cudaError_t batch(const BatchLaunchParams &p, int set, cudaStream_t s) {
         const unsigned tiles = p.starts[p.count];
         if (p.count <= 0 || p.count > BATCH_LAUNCH_MAX || tiles == 0) return cudaErrorInvalidValue;
@@ -728,6 +794,25 @@ struct StepLaunch {
         return cudaGetLastError();
     }
 };
+
+// The launcher table of one storage format (exported by its translation unit).
+template <class S>
+StepOps make_step_ops() {
+    using L = StepLaunch<S>;
+    StepOps o;
+    o.step = &L::step;
+    o.batch = &L::batch;
+    o.batch_pair = &L::batch_pair;
+    o.tma_prepare = &L::tma_prepare;
+    o.stream_only = &L::stream_only;
+    o.velocity = &L::velocity;
+    o.init_uniform = &L::init_uniform;
+    o.init_field = &L::init_field;
+    o.export_aos = &L::export_aos;
+    o.import_aos = &L::import_aos;
+    o.mass_momentum = &L::mass_momentum;
+    return o;
+}
 
 }  // namespace LBM_ARITH_NS
 }  // namespace lbm
