@@ -2,10 +2,13 @@
 //
 // Two schedules, chosen per batch by LBM_BatchAutotune from measurements:
 //   fused - one kernel launch per step for up to 64 grids of one collision
-//           operator (k_step_batch: the grids' tiles concatenated, each grid's
-//           arguments read from the kernel parameter);
-//   graph - every grid's own fused step kernel (k_step, the grid's tile
-//           shape), the grids spread over a few streams that run
+//           operator: the grids' tiles concatenated, each block reading its
+//           grid's entry from a table in device memory into shared memory
+//           (k_step_batch_pair, two cells per thread; batches holding an
+//           FP64 grid or an odd NX take the one-cell k_step_batch, whose
+//           entries are in the kernel parameter);
+//   graph - every grid's own fused step kernel (k_step_pair or k_step, the
+//           grid's tile shape), the grids spread over a few streams that run
 //           concurrently.
 // Either way a 32-step chunk is captured once as a CUDA graph and replayed
 // while the arguments stay the same (one graph launch per chunk), and every
@@ -38,6 +41,15 @@ struct LBMBatch {
     int count = 0;
     int storage = LBM_STORAGE_FP32;
     int mode = MODE_FUSED;
+    // every grid can take the paired kernels (FP32 / FP16 / BF16, even NX)
+    bool pair = false;
+    // the paired fused schedule's grid entries in group order: host copies,
+    // what was last uploaded, and the device tables, one per buffer parity
+    std::vector<BatchGridDev> tab[2];
+    std::vector<BatchGridDev> tab_uploaded[2];
+    BatchGridDev *dev_tab[2] = {nullptr, nullptr};
+    std::vector<BatchPairParams> pparams[2];
+    std::vector<BatchPairParams> graph_pparams[2];
     std::vector<LBMGrid *> grids;
     std::vector<int> lbx;                 // tile width exponent per grid
     std::vector<cudaEvent_t> grid_done;   // recorded on each grid's stream
@@ -61,6 +73,13 @@ struct LBMBatch {
     std::vector<StepArgs> graph_args[2];
     std::vector<int> graph_lbx;
 };
+
+// the tile of a grid in cells: pair batches 2 << lbx by 128 >> lbx (lbx 5..7),
+// one-cell batches 1 << lbx by 256 >> lbx (lbx 5..8)
+static int tile_x_cells(const LBMBatch &b, int lbx) { return b.pair ? 2 << lbx : 1 << lbx; }
+static int tile_y_cells(const LBMBatch &b, int lbx) { return b.pair ? 128 >> lbx : 256 >> lbx; }
+static int lbx_min() { return 5; }
+static int lbx_max(const LBMBatch &b) { return b.pair ? 7 : 8; }
 
 namespace {
 
@@ -104,6 +123,17 @@ bool same_params(const std::vector<BatchLaunchParams> &x, const std::vector<Batc
                 a.e[j].lbx != b.e[j].lbx || a.e[j].tiles_x != b.e[j].tiles_x ||
                 a.e[j].tiles_y != b.e[j].tiles_y)
                 return false;
+    }
+    return true;
+}
+
+bool same_pair_params(const std::vector<BatchPairParams> &x,
+                      const std::vector<BatchPairParams> &y) {
+    if (x.size() != y.size()) return false;
+    for (size_t i = 0; i < x.size(); i++) {
+        if (x[i].grids != y[i].grids || x[i].count != y[i].count) return false;
+        for (int j = 0; j <= x[i].count; j++)
+            if (x[i].starts[j] != y[i].starts[j]) return false;
     }
     return true;
 }
@@ -198,9 +228,14 @@ bool build_params(LBMBatch &b, const std::vector<StepArgs> &a, std::vector<Batch
 // the grid's fused step kernel with the batch's tile shape for it
 cudaError_t grid_step(LBMBatch &b, int i, const StepArgs &a, cudaStream_t s) {
     GridImpl t = *impl(b.grids[i]);
-    t.bx = 1 << b.lbx[i];
-    t.by = 256 >> b.lbx[i];
-    t.cpt = 1;
+    if (b.pair) {
+        t.cpt = 2;
+        t.pbx = 1 << b.lbx[i];
+    } else {
+        t.bx = 1 << b.lbx[i];
+        t.by = 256 >> b.lbx[i];
+        t.cpt = 1;
+    }
     t.minb = 4;
     const int op = grid_op(b.grids[i]);
     return launch_step(t, a, true, op, b.grids[i]->useSmagorinsky == 1, false, s);
@@ -231,6 +266,92 @@ bool step_fused(LBMBatch &b, const std::vector<BatchLaunchParams> &p, const std:
     return true;
 }
 
+// The paired kernel's pointer table for step arguments a (element size elem).
+PairTable pair_table_of(const StepArgs &a, size_t elem) {
+    PairTable t;
+    const char *src = static_cast<const char *>(a.src);
+    char *dst = static_cast<char *>(a.dst);
+    const long long plane = (long long)a.nx * a.ny;
+    static const int ex[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+    static const int ey[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
+    static const int ez[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
+    for (int i = 0; i < 19; i++) {
+        const long long own = (long long)i * a.n;
+        const long long shift = ex[i] + ey[i] * (long long)a.nx + ez[i] * plane;
+        t.own[i] = src + own * (long long)elem;
+        t.pull[i] = src + (own - shift) * (long long)elem;
+        t.dst[i] = dst + own * (long long)elem;
+    }
+    t.nz = make_float2(-0.0f, -0.0f);
+    return t;
+}
+
+BatchGridDev pair_entry(LBMBatch &b, int i, const StepArgs &a) {
+    BatchGridDev e;
+    memset(&e, 0, sizeof(e));  // padding too: entries are compared bytewise
+    e.a = a;
+    e.t = pair_table_of(a, impl(b.grids[i])->elem);
+    e.combo = combo_of(b.grids[i]);
+    e.lbx = b.lbx[i];
+    e.tiles_x = (impl(b.grids[i])->nx + tile_x_cells(b, e.lbx) - 1) / tile_x_cells(b, e.lbx);
+    e.tiles_y = (impl(b.grids[i])->ny + tile_y_cells(b, e.lbx) - 1) / tile_y_cells(b, e.lbx);
+    return e;
+}
+
+// The paired entries of every grid for per-grid step arguments a, in group
+// order (the grids of group 0, then of group 1, ...), copied to device table
+// `parity` when they differ from what it holds.
+bool upload_pair_table(LBMBatch &b, const std::vector<StepArgs> &a, int parity) {
+    std::vector<BatchGridDev> &t = b.tab[parity];
+    t.clear();
+    for (const std::vector<int> &grp : b.groups)
+        for (int i : grp) t.push_back(pair_entry(b, i, a[i]));
+    const size_t bytes = sizeof(BatchGridDev) * t.size();
+    if (b.tab_uploaded[parity].size() == t.size() &&
+        memcmp(b.tab_uploaded[parity].data(), t.data(), bytes) == 0)
+        return true;
+    if (fail(b.grids[0], cudaMemcpyAsync(b.dev_tab[parity], t.data(), bytes,
+                                         cudaMemcpyHostToDevice, b.stream)))
+        return false;
+    b.tab_uploaded[parity] = t;
+    return true;
+}
+
+// The paired launch of every group over device table `parity` (made by
+// upload_pair_table with the same groups).
+bool build_pair_params(LBMBatch &b, int parity, std::vector<BatchPairParams> &out,
+                       std::vector<int> &sets) {
+    out.assign(b.groups.size(), BatchPairParams{});
+    sets.assign(b.groups.size(), BATCH_SET_ALL);
+    size_t base = 0;
+    for (size_t gi = 0; gi < b.groups.size(); gi++) {
+        const std::vector<int> &grp = b.groups[gi];
+        unsigned used = 0;
+        long long total = 0;
+        for (size_t j = 0; j < grp.size(); j++) {
+            const BatchGridDev &e = b.tab[parity][base + j];
+            out[gi].starts[j] = (unsigned)total;
+            total += (long long)e.tiles_x * e.tiles_y * impl(b.grids[grp[j]])->nz;
+            used |= 1u << e.combo;
+        }
+        if (total > 0x7fffffffLL) return false;
+        out[gi].starts[grp.size()] = (unsigned)total;
+        out[gi].count = (int)grp.size();
+        out[gi].grids = b.dev_tab[parity] + base;
+        sets[gi] = set_of(used);
+        base += grp.size();
+    }
+    return true;
+}
+
+bool step_fused_pair(LBMBatch &b, const std::vector<BatchPairParams> &p,
+                     const std::vector<int> &sets) {
+    for (size_t gi = 0; gi < p.size(); gi++)
+        if (fail(b.grids[0], launch_step_batch_pair(b.storage, p[gi], sets[gi], b.stream)))
+            return false;
+    return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -252,7 +373,10 @@ LBMBatch *LBM_BatchCreate(LBMGrid **grids, int count) {
     b->count = count;
     b->storage = storage;
     b->grids.assign(grids, grids + count);
-    b->lbx.assign(count, 5);  // 32 x 8 tiles, the single-grid default
+    b->pair = storage != LBM_STORAGE_FP64;
+    for (int i = 0; i < count; i++)
+        if (impl(grids[i])->nx % 2 != 0 || impl(grids[i])->n >= (1ll << 31)) b->pair = false;
+    b->lbx.assign(count, 5);  // 64 x 4 (pair) or 32 x 8 tiles, the single-grid defaults
     b->grid_done.assign(count, nullptr);
     bool good = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess;
     good = good && cudaEventCreateWithFlags(&b->batch_done, cudaEventDisableTiming) == cudaSuccess;
@@ -264,6 +388,8 @@ LBMBatch *LBM_BatchCreate(LBMGrid **grids, int count) {
     }
     for (int i = 0; good && i < count; i++)
         good = cudaEventCreateWithFlags(&b->grid_done[i], cudaEventDisableTiming) == cudaSuccess;
+    for (int p = 0; good && b->pair && p < 2; p++)
+        good = cudaMalloc(&b->dev_tab[p], sizeof(BatchGridDev) * (size_t)count) == cudaSuccess;
     if (!good) {
         LBM_BatchFree(b);
         return nullptr;
@@ -286,6 +412,8 @@ void LBM_BatchFree(LBMBatch *b) {
         if (b->side_done[s]) cudaEventDestroy(b->side_done[s]);
     }
     if (b->stream) cudaStreamDestroy(b->stream);
+    for (int p = 0; p < 2; p++)
+        if (b->dev_tab[p]) cudaFree(b->dev_tab[p]);
     delete b;
 }
 
@@ -324,9 +452,16 @@ int LBM_BatchRun(LBMBatch *b, int nSteps, const float *inlet) {
         b->args[0][i] = step_of(g, I.pop[I.gbuf], I.pop[1 - I.gbuf], inlet + 3 * i);
         b->args[1][i] = step_of(g, I.pop[1 - I.gbuf], I.pop[I.gbuf], inlet + 3 * i);
     }
-    if (b->mode == MODE_FUSED && (!build_params(*b, b->args[0], b->params[0], b->sets) ||
-                                  !build_params(*b, b->args[1], b->params[1], b->sets)))
+    if (b->mode == MODE_FUSED && b->pair) {
+        if (!upload_pair_table(*b, b->args[0], 0) || !upload_pair_table(*b, b->args[1], 1))
+            return LBM_ERR_CUDA;
+        if (!build_pair_params(*b, 0, b->pparams[0], b->sets) ||
+            !build_pair_params(*b, 1, b->pparams[1], b->sets))
+            return LBM_ERR_INVALID_ARGUMENT;
+    } else if (b->mode == MODE_FUSED && (!build_params(*b, b->args[0], b->params[0], b->sets) ||
+                                         !build_params(*b, b->args[1], b->params[1], b->sets))) {
         return LBM_ERR_INVALID_ARGUMENT;
+    }
 
     // the batch waits for every grid's queued work
     for (int i = 0; i < n; i++) {
@@ -339,13 +474,19 @@ int LBM_BatchRun(LBMBatch *b, int nSteps, const float *inlet) {
     auto run = [&](int k) {
         if (b->mode == MODE_GRAPH) return k == 0 || steps_graph(*b, b->args, k);
         for (int j = 0; j < k; j++)
-            if (!step_fused(*b, b->params[j & 1], b->sets)) return false;
+            if (!(b->pair ? step_fused_pair(*b, b->pparams[j & 1], b->sets)
+                          : step_fused(*b, b->params[j & 1], b->sets)))
+                return false;
         return true;
     };
     int left = steps;
     if (left >= kChunk) {
         bool stale = !b->graph || b->graph_mode != b->mode;
-        if (!stale && b->mode == MODE_FUSED)
+        if (!stale && b->mode == MODE_FUSED && b->pair)
+            stale = b->graph_sets != b->sets ||
+                    !same_pair_params(b->graph_pparams[0], b->pparams[0]) ||
+                    !same_pair_params(b->graph_pparams[1], b->pparams[1]);
+        else if (!stale && b->mode == MODE_FUSED)
             stale = b->graph_sets != b->sets || !same_params(b->graph_params[0], b->params[0]) ||
                     !same_params(b->graph_params[1], b->params[1]);
         if (!stale && b->mode == MODE_GRAPH)
@@ -367,6 +508,8 @@ int LBM_BatchRun(LBMBatch *b, int nSteps, const float *inlet) {
             b->graph_mode = b->mode;
             b->graph_params[0] = b->params[0];
             b->graph_params[1] = b->params[1];
+            b->graph_pparams[0] = b->pparams[0];
+            b->graph_pparams[1] = b->pparams[1];
             b->graph_sets = b->sets;
             b->graph_args[0] = b->args[0];
             b->graph_args[1] = b->args[1];
@@ -427,18 +570,37 @@ int LBM_BatchAutotune(LBMBatch *b, int trialLaunches) {
     std::vector<int> lbx_fused(n, 5), lbx_graph(n, 5);
     for (int i = 0; good && i < n; i++) {
         float best_f = 1e30f, best_g = 1e30f;
-        for (int l = 5; good && l <= 8; l++) {
-            BatchLaunchParams p{};
-            p.e[0] = make_entry(b->grids[i], l, a[i]);
-            p.starts[0] = 0;
-            p.starts[1] = (unsigned)units_of(p.e[0], impl(b->grids[i])->nz);
-            p.count = 1;
-            const int set = set_of(1u << p.e[0].combo);
-            const float mf = timed([&] {
-                return !fail(g0, launch_step_batch(b->storage, p, set, b->stream));
-            });
-            if (good && mf < best_f * 0.98f) best_f = mf, lbx_fused[i] = l;
+        for (int l = lbx_min(); good && l <= lbx_max(*b); l++) {
             b->lbx[i] = l;
+            float mf = 1e30f;
+            if (b->pair) {
+                // this grid alone through the paired fused kernel, its entry
+                // in device table 0
+                const BatchGridDev e = pair_entry(*b, i, a[i]);
+                good = !fail(g0, cudaMemcpyAsync(b->dev_tab[0], &e, sizeof(e),
+                                                  cudaMemcpyHostToDevice, b->stream)) &&
+                       !fail(g0, cudaStreamSynchronize(b->stream));
+                BatchPairParams p{};
+                p.grids = b->dev_tab[0];
+                p.starts[0] = 0;
+                p.starts[1] = (unsigned)((long long)e.tiles_x * e.tiles_y * impl(b->grids[i])->nz);
+                p.count = 1;
+                const int set = set_of(1u << e.combo);
+                mf = timed([&] {
+                    return !fail(g0, launch_step_batch_pair(b->storage, p, set, b->stream));
+                });
+            } else {
+                BatchLaunchParams p{};
+                p.e[0] = make_entry(b->grids[i], l, a[i]);
+                p.starts[0] = 0;
+                p.starts[1] = (unsigned)units_of(p.e[0], impl(b->grids[i])->nz);
+                p.count = 1;
+                const int set = set_of(1u << p.e[0].combo);
+                mf = timed([&] {
+                    return !fail(g0, launch_step_batch(b->storage, p, set, b->stream));
+                });
+            }
+            if (good && mf < best_f * 0.98f) best_f = mf, lbx_fused[i] = l;
             const float mg = timed([&] { return !fail(g0, grid_step(*b, i, a[i], b->stream)); });
             if (good && mg < best_g * 0.98f) best_g = mg, lbx_graph[i] = l;
         }
@@ -448,10 +610,18 @@ int LBM_BatchAutotune(LBMBatch *b, int trialLaunches) {
     if (good) {
         b->lbx = lbx_fused;
         make_groups(*b);
-        std::vector<BatchLaunchParams> p;
         std::vector<int> sets;
-        good = build_params(*b, a, p, sets);
-        ms_fused = timed([&] { return step_fused(*b, p, sets); });
+        if (b->pair) {
+            std::vector<BatchPairParams> p;
+            b->tab_uploaded[0].clear();  // device table 0 was overwritten above
+            good = upload_pair_table(*b, a, 0) && build_pair_params(*b, 0, p, sets);
+            ms_fused = timed([&] { return step_fused_pair(*b, p, sets); });
+            b->tab_uploaded[0].clear();  // holds the trial arguments now
+        } else {
+            std::vector<BatchLaunchParams> p;
+            good = build_params(*b, a, p, sets);
+            ms_fused = timed([&] { return step_fused(*b, p, sets); });
+        }
     }
     if (good) {
         b->lbx = lbx_graph;
@@ -472,16 +642,16 @@ int LBM_BatchAutotune(LBMBatch *b, int trialLaunches) {
 
 int LBM_BatchGetTile(LBMBatch *b, int index, int *tileX, int *tileY) {
     if (!b || index < 0 || index >= b->count || !tileX || !tileY) return LBM_ERR_INVALID_ARGUMENT;
-    *tileX = 1 << b->lbx[index];
-    *tileY = 256 >> b->lbx[index];
+    *tileX = tile_x_cells(*b, b->lbx[index]);
+    *tileY = tile_y_cells(*b, b->lbx[index]);
     return LBM_OK;
 }
 
 int LBM_BatchSetTile(LBMBatch *b, int index, int tileX) {
     if (!b || index < 0 || index >= b->count) return LBM_ERR_INVALID_ARGUMENT;
     int lbx = -1;
-    for (int k = 5; k <= 8; k++)
-        if (tileX == (1 << k)) lbx = k;
+    for (int k = lbx_min(); k <= lbx_max(*b); k++)
+        if (tileX == tile_x_cells(*b, k)) lbx = k;
     if (lbx < 0) return LBM_ERR_INVALID_ARGUMENT;
     if (b->lbx[index] != lbx) drop_graph(*b);
     b->lbx[index] = lbx;
@@ -501,7 +671,7 @@ long long LBM_BatchTilesPerStep(LBMBatch *b) {
     if (!b) return 0;
     long long total = 0;
     for (int i = 0; i < b->count; i++) {
-        const int bx = 1 << b->lbx[i], by = 256 >> b->lbx[i];
+        const int bx = tile_x_cells(*b, b->lbx[i]), by = tile_y_cells(*b, b->lbx[i]);
         const GridImpl &I = *impl(b->grids[i]);
         total += (long long)((I.nx + bx - 1) / bx) * ((I.ny + by - 1) / by) * I.nz;
     }

@@ -64,7 +64,7 @@ size_t elem_size(int storage) {
 void default_block(GridImpl &I) {
     I.bx = 32;
     I.by = 8;
-    I.cpt = 1;
+    I.cpt = 2;
     I.pbx = 32;
     I.minb = 4;
     const char *cenv = getenv("LBM_CPT");

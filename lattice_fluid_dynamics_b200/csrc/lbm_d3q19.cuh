@@ -65,38 +65,13 @@ enum : uint8_t {
     FLAG_BOUNDARY = 0x4     // cell owns at least one boundary link
 };
 
-// Loads that the compiler must issue where they are written (asm volatile):
-// the paired MRT + Smagorinsky step reads the pulled populations a second
-// time, from L1, instead of keeping them in registers.
-__device__ __forceinline__ float ldv_f32(const float *p) {
-    float v;
-    asm volatile("ld.global.nc.f32 %0, [%1];" : "=f"(v) : "l"(p));
-    return v;
-}
-__device__ __forceinline__ float2 ldv_f32x2(const float *p) {
-    float2 v;
-    asm volatile("ld.global.nc.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
-    return v;
-}
-__device__ __forceinline__ unsigned short ldv_u16(const void *p) {
-    unsigned short v;
-    asm volatile("ld.global.nc.u16 %0, [%1];" : "=h"(v) : "l"(p));
-    return v;
-}
-__device__ __forceinline__ unsigned ldv_u32(const void *p) {
-    unsigned v;
-    asm volatile("ld.global.nc.u32 %0, [%1];" : "=r"(v) : "l"(p));
-    return v;
-}
-
 // ---------------------------------------------------------------------
 // Population storage formats.  R is the collision arithmetic type.
 // FP16/BF16 keep the deviation f_i - w_i (w_i in FP32).
 // ---------------------------------------------------------------------
 // load2/store2 move the populations of two neighbouring cells (p must be
 // aligned to two elements).  `load` reads global memory through the
-// read-only path; `lds` reads a population staged in shared memory;
-// reload / reload2 are load / load2 issued where written (see ldv_f32).
+// read-only path; `lds` reads a population staged in shared memory.
 struct StoreF32 {
     using T = float;
     using R = float;
@@ -110,12 +85,6 @@ struct StoreF32 {
     }
     static __device__ __forceinline__ void store2(T *p, R a, R b, int) {
         *reinterpret_cast<float2 *>(p) = make_float2(a, b);
-    }
-    static __device__ __forceinline__ R reload(const T *p, int) { return ldv_f32(p); }
-    static __device__ __forceinline__ void reload2(const T *p, int, R &a, R &b) {
-        const float2 v = ldv_f32x2(p);
-        a = v.x;
-        b = v.y;
     }
 };
 struct StoreF64 {
@@ -154,14 +123,6 @@ struct StoreF16 {
         *reinterpret_cast<__half2 *>(p) =
             __halves2half2(__float2half_rn(a - wgt<float>(i)), __float2half_rn(b - wgt<float>(i)));
     }
-    static __device__ __forceinline__ R reload(const T *p, int i) {
-        return __half2float(__ushort_as_half(ldv_u16(p))) + wgt<float>(i);
-    }
-    static __device__ __forceinline__ void reload2(const T *p, int i, R &a, R &b) {
-        const unsigned u = ldv_u32(p);
-        a = __half2float(__ushort_as_half((unsigned short)(u & 0xffffu))) + wgt<float>(i);
-        b = __half2float(__ushort_as_half((unsigned short)(u >> 16))) + wgt<float>(i);
-    }
 };
 struct StoreBF16 {
     using T = __nv_bfloat16;
@@ -183,14 +144,6 @@ struct StoreBF16 {
     static __device__ __forceinline__ void store2(T *p, R a, R b, int i) {
         *reinterpret_cast<__nv_bfloat162 *>(p) = __halves2bfloat162(
             __float2bfloat16_rn(a - wgt<float>(i)), __float2bfloat16_rn(b - wgt<float>(i)));
-    }
-    static __device__ __forceinline__ R reload(const T *p, int i) {
-        return __bfloat162float(__ushort_as_bfloat16(ldv_u16(p))) + wgt<float>(i);
-    }
-    static __device__ __forceinline__ void reload2(const T *p, int i, R &a, R &b) {
-        const unsigned u = ldv_u32(p);
-        a = __bfloat162float(__ushort_as_bfloat16((unsigned short)(u & 0xffffu))) + wgt<float>(i);
-        b = __bfloat162float(__ushort_as_bfloat16((unsigned short)(u >> 16))) + wgt<float>(i);
     }
 };
 

@@ -26,10 +26,8 @@
 //
 // Pairs that hold a solid body cell take the scalar per-cell code; Zou-He
 // cells and guard resets stay on the paired path (per-lane rewrite before
-// the moments, per-lane select after the collision), except for MRT +
-// Smagorinsky, whose two-pass form (below) takes only pairs without a
-// Zou-He lane or a boundary link.  Included by lbm_step.cuh after the
-// per-cell pieces it uses.
+// the moments, per-lane select after the collision).  Included by
+// lbm_step.cuh after the per-cell pieces it uses.
 #pragma once
 
 #include "lbm_d3q19.cuh"
@@ -145,7 +143,7 @@ __device__ __forceinline__ void pstress(const P (&F)[19], const P (&fe)[19], P &
 // formed in index order and added at once to each sum it belongs to, so each
 // sum receives its terms in the order stress() adds them and no array of
 // equilibria stays live.  feq_i is evaluated as in pequilibria; f_i is
-// get(i), read from the registers or a second time from memory.
+// get(i).
 template <class Get>
 __device__ __forceinline__ void pstress_streamed(Get get, P rho, P ux, P uy, P uz, P u2, P nz,
                                                  P &Pxx, P &Pyy, P &Pzz, P &Pxy, P &Pxz, P &Pyz) {
@@ -457,48 +455,23 @@ __device__ __forceinline__ void pair_collide_fluid(float (&fa)[19], float (&fb)[
     }
 }
 
-// MRT + Smagorinsky on a pair in two passes, for pairs with no Zou-He lane
-// and no boundary link: the first pass consumes the pulled populations F for
-// the moments and the MRT forward transform, the second reads them again
-// (reload(i), from L1) for the Smagorinsky stress.  The arithmetic of each
-// lane is pair_collide_fluid's; only the order of independent parts
-// changes, so the populations are not live across the stress and the
-// kernel fits fewer registers.
-template <class Reload>
-__device__ __forceinline__ void pair_collide_mrt_smag(const P (&F)[19], Reload reload, float tau,
-                                                      float smag18, P nz, P (&fn)[19],
-                                                      bool &resetA, bool &resetB) {
-    P rho, ux, uy, uz, u2;
-    pmoments(F, rho, ux, uy, uz);
-    P m[19];
-    pmrt_forward(F, nz, m);
-    pvelocity_guard(rho, ux, uy, uz, u2, nz, resetA, resetB);
-    P Pxx, Pyy, Pzz, Pxy, Pxz, Pyz;
-    pstress_streamed(reload, rho, ux, uy, uz, u2, nz, Pxx, Pyy, Pzz, Pxy, Pxz, Pyz);
-    const P omega = psmag_omega(Pxx, Pyy, Pzz, Pxy, Pxz, Pyz, rho, tau, smag18, nz);
-    pmrt_relax_inverse(m, rho, ux, uy, uz, u2, omega, nz, fn);
-#pragma unroll
-    for (int i = 0; i < 19; i++) {
-        if (resetA) fn[i].x = wgt<float>(i);
-        if (resetB) fn[i].y = wgt<float>(i);
-    }
-}
-
 // ---------------------------------------------------------------------------
 // The kernels
 // ---------------------------------------------------------------------------
 constexpr int PAIR_THREADS = 128;  // threads per block (two cells each)
 // Blocks resident per SM the paired kernels are compiled for (register cap
-// 65536 / (PAIR_THREADS * blocks)): 6 (80 registers) for the operators that
-// fit it, 5 (96 registers) for BGK / regularized with Smagorinsky, which
-// would spill more than a hundred bytes at 80, and for batched launches that
-// mix operators.  LBM_PAIR_MINB overrides all of them (measurements).
+// 65536 / (PAIR_THREADS * blocks)), measured on B200 at 256x128x128: 7 (72
+// registers) for the operators without Smagorinsky (FP32 BGK 41.0k, FP16
+// BGK 53.1k MLUPS against 41.0k / 48.7k at 6), 6 (80 registers) with it (MRT
+// + Smagorinsky 31.8k against 30.7k at 5 and 31.6k at 7; regularized +
+// Smagorinsky 37.3k against 34.8k at 5).  LBM_PAIR_MINB overrides all of them
+// (measurements).
 template <int OP, bool SMAG>
 __host__ __device__ constexpr int pair_minb() {
 #ifdef LBM_PAIR_MINB
     return LBM_PAIR_MINB;
 #else
-    return (SMAG && OP != OP_MRT) ? 5 : 6;
+    return SMAG ? 6 : 7;
 #endif
 }
 __host__ __device__ constexpr int pair_minb_set(int set) {
@@ -506,7 +479,7 @@ __host__ __device__ constexpr int pair_minb_set(int set) {
          : set == BATCH_SET_REG ? pair_minb<OP_REG, false>()
          : set == BATCH_SET_MRT ? pair_minb<OP_MRT, false>()
          : set == BATCH_SET_MRT_SMAG ? pair_minb<OP_MRT, true>()
-         : 5;
+         : 6;
 }
 
 // Where the scalar fallback parks the second cell of a pair (one array per
@@ -608,44 +581,6 @@ __device__ __forceinline__ void step_pair(const StepArgs &a, const PairTable &t,
     if (solidA == 1 || solidB == 1) {
         // a body cell in the pair
         scalar_pair();
-    } else if constexpr (OP == OP_MRT && SMAG) {
-        const bool plain = !((flagA | flagB) & FLAG_BOUNDARY) && x0 != 0 && x0 + 2 != a.nx;
-        if (plain) {
-            // the two-pass form: the second pass reads the pulled values again
-            auto reload = [&](int i) -> P {
-                float va, vb;
-                if (!FUSED) {
-                    S::reload2(static_cast<const T *>(t.own[i]) + cell0, i, va, vb);
-                } else if (interior_row) {
-                    const T *p = static_cast<const T *>(t.pull[i]) + cell0;
-                    if (cx(i) == 0) {
-                        S::reload2(p, i, va, vb);
-                    } else {
-                        va = S::reload(p, i);
-                        vb = S::reload(p + 1, i);
-                    }
-                } else {
-                    // a y / z face row: the wrapped or clamped source rows;
-                    // x0 - e_x and x0 + 1 - e_x lie inside the grid here
-                    const Rows rw = neighbour_rows(a, y, z);
-                    const T *src = static_cast<const T *>(a.src) + (long long)i * a.n +
-                                   rw.y[1 - cy(i)] + rw.z[1 - cz(i)] - cx(i);
-                    va = S::reload(src + x0, i);
-                    vb = S::reload(src + x0 + 1, i);
-                }
-                return make_float2(va, vb);
-            };
-            P F[19];
-#pragma unroll
-            for (int i = 0; i < 19; i++) F[i] = make_float2(fa[i], fb[i]);
-            P fn[19];
-            bool resetA, resetB;
-            pair_collide_mrt_smag(F, reload, a.tau, a.smag18, t.nz, fn, resetA, resetB);
-            resets = (int)resetA + (int)resetB;
-            store_pair(fn);
-        } else {
-            scalar_pair();
-        }
     } else {
         P fn[19];
         bool resetA, resetB;

@@ -33,14 +33,19 @@ import numpy as np
 from . import capi, geometry
 
 
-def build_grid(inst: dict, storage: str = "fp32") -> capi.Grid:
-    """One instance through the reference's API: viscosity from Re with the
-    reference's 0.52 tau clamp (simulation/src/main.c:447-460), mesh body,
-    periodic y/z, uniform inlet flow."""
+def build_grid(inst: dict, storage: str = "fp32", tau_clamp: bool = False) -> capi.Grid:
+    """One instance through the reference's API: mesh body, periodic y/z,
+    uniform inlet flow.  tau = 3 U L / Re + 1/2 is set directly, so the
+    instance runs at the Reynolds number it was drawn with (the sweep's
+    contract: tau set for Re in [100, 2000]); with tau_clamp the viscosity
+    goes through the reference driver's rule instead, whose 0.52 tau floor
+    (simulation/src/main.c:447-460) lowers the Re that runs."""
     nx, ny, nz = inst["dims"]
     _, nu, _, _ = capi.reynolds_to_tau(inst["U"], inst["length"], inst["Re"])
     g = capi.Grid(nx, ny, nz, nu, storage=storage)
     g.set(useRegularized=1 if inst["op"] == "reg" else 0, periodicYZ=1)
+    if not tau_clamp:
+        g.set(tau=geometry.reynolds_tau(inst["U"], inst["length"], inst["Re"]))
     g.set_solid_mesh(inst["triangles"], inst["bbox"])
     g.initialize_flow(inst["U"])
     return g
@@ -87,7 +92,7 @@ def merge_ranks(results: list) -> dict:
     ms = max(r["ms"] for r in results)
     cells = sum(r["cells_total"] for r in results)
     total = cells * first["steps"]
-    out = {k: first[k] for k in ("steps", "seed", "storage")}
+    out = {k: first[k] for k in ("steps", "seed", "storage", "tau_clamp") if k in first}
     out.update({
         "instances": sum(r["instances"] for r in results), "ranks": len(results),
         "cells_total": cells, "ms": ms, "mlups": total / (ms * 1e-3) / 1e6,
@@ -104,7 +109,7 @@ def merge_ranks(results: list) -> dict:
 
 def run_sweep(count: int = 64, steps: int = 3000, seed: int = 1, autotune: bool = True,
               solo: bool = True, storage: str = "fp32", warmup: int = 0,
-              indices=None) -> dict:
+              indices=None, tau_clamp: bool = False) -> dict:
     """The sweep of `count` instances from `seed`, or of the subset
     `indices` of them (a rank's shard); per-instance results keep the
     instance's index in the full sweep."""
@@ -113,7 +118,7 @@ def run_sweep(count: int = 64, steps: int = 3000, seed: int = 1, autotune: bool 
     insts = [insts[k] for k in index]
     count = len(insts)
     t0 = time.perf_counter()
-    grids = [build_grid(i, storage) for i in insts]
+    grids = [build_grid(i, storage, tau_clamp) for i in insts]
     setup_s = time.perf_counter() - t0
     areas = [g.projected_area(0) for g in grids]
     cells = np.array([np.prod(i["dims"]) for i in insts], np.int64)
@@ -129,6 +134,7 @@ def run_sweep(count: int = 64, steps: int = 3000, seed: int = 1, autotune: bool 
     total = int(cells.sum()) * steps
     res = {
         "instances": count, "steps": steps, "seed": seed, "storage": storage,
+        "tau_clamp": tau_clamp,
         "cells_total": int(cells.sum()), "ms": ms,
         "mlups": total / (ms * 1e-3) / 1e6,
         "gb_per_s": total * grids[0].bytes_per_update() / (ms * 1e-3) / 1e9,
@@ -140,13 +146,14 @@ def run_sweep(count: int = 64, steps: int = 3000, seed: int = 1, autotune: bool 
         res["per_instance"].append({
             "index": index[k], "dims": list(inst["dims"]), "kind": inst["kind"], "op": inst["op"],
             "U": inst["U"], "Re": inst["Re"], "tau": float(g.s.tau),
+            "Re_run": inst["U"] * inst["length"] / ((float(g.s.tau) - 0.5) / 3.0),
             "tile": list(batch.tile(k)), "area": areas[k],
             "cd": drag_coefficient(g, inst["U"], areas[k]),
             "guard_resets": g.guard_resets(),
         })
     batch.close()
     if solo:
-        sgrids = [build_grid(i, storage) for i in insts]
+        sgrids = [build_grid(i, storage, tau_clamp) for i in insts]
 
         def solo_all():
             for inst, g in zip(insts, sgrids):
@@ -183,6 +190,8 @@ def main(argv=None) -> int:
     ap.add_argument("--storage", default="fp32")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-solo", action="store_true")
+    ap.add_argument("--tau-clamp", action="store_true",
+                    help="viscosity through the reference driver's rule (tau >= 0.52)")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -198,7 +207,7 @@ def main(argv=None) -> int:
         dims = [i["dims"] for i in geometry.sweep_instances(a.seed, a.count)]
         indices = shard(dims, world, rank)
     res = run_sweep(a.count, a.steps, a.seed, not a.no_autotune, not a.no_solo, a.storage,
-                    indices=indices)
+                    indices=indices, tau_clamp=a.tau_clamp)
     if world > 1:
         gathered = [None] * world
         dist.all_gather_object(gathered, res)
@@ -211,6 +220,9 @@ def main(argv=None) -> int:
     for p in res["per_instance"]:
         tiles[f"{p['tile'][0]}x{p['tile'][1]}"] = tiles.get(f"{p['tile'][0]}x{p['tile'][1]}", 0) + 1
     summary["tiles"] = tiles
+    summary["instances_with_guard_resets"] = sum(p["guard_resets"] > 0 for p in res["per_instance"])
+    summary["re_run_range"] = [min(p["Re_run"] for p in res["per_instance"]),
+                               max(p["Re_run"] for p in res["per_instance"])]
     print(json.dumps(summary))
     if a.out:
         with open(a.out, "w") as fh:
