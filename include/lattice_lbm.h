@@ -580,6 +580,51 @@ typedef struct {
  * frames), Strouhal at the end.  Returns LBM_OK or an LBM_ERR_* code. */
 int LBM_TunnelRun(const LBMTunnelOptions *options, LBMTunnelResult *result);
 
+/* ---------------------------------------------------------------------
+ * Super-resolution upscaling of the velocity field: the reference's
+ * SR_* API (simulation/lib/superres.h, simulation/src/superres.c:178-285,
+ * simulation/shaders/superres_upscale.comp).  Per coarse cell, the 3x3x3
+ * neighbourhood of (ux, uy, uz, rho) -- clamped at the grid faces,
+ * normalised by the channel mean and std -- feeds an MLP 108 -> 128 -> 128
+ * -> 128 -> 32 (ReLU between layers) whose output corrects a trilinear
+ * estimate of the 2x2x2 fine cells; the sum is denormalised and written to
+ * the fine field (2x the coarse size in each direction).  The MLP runs on
+ * the tensor cores with BF16 operands and FP32 accumulation.
+ * ------------------------------------------------------------------- */
+typedef struct LBMSuperRes LBMSuperRes;
+
+/* SR_Create (superres.c:178-236): weights from an LTWS file (magic "LTWS",
+ * version, parameter count, then per parameter its rank, shape and FP32
+ * values: b0, W0, b1, W1, b2, W2, b3, W3 -- superres.c:43-101), the channel
+ * mean[4] and std[4] from normPath (two FP32 vec4; a missing file means mean
+ * 0 and std 1, as the reference does, superres.c:103-127).  NULL when the
+ * weights cannot be read or do not have the 51,104 values of this network,
+ * or when an allocation fails. */
+LBMSuperRes *LBM_SuperResCreate(int coarseX, int coarseY, int coarseZ, const char *weightsPath,
+                                const char *normPath);
+/* The same from host arrays: `weights` holds the 51,104 values in the file's
+ * order, mean and std 4 values each. */
+LBMSuperRes *LBM_SuperResCreateFromArrays(int coarseX, int coarseY, int coarseZ,
+                                          const float *weights, long long count,
+                                          const float *mean, const float *std);
+/* SR_Free (superres.c:238-244); accepts NULL. */
+void LBM_SuperResFree(LBMSuperRes *sr);
+/* SR_Upscale (superres.c:246-274): `coarseVelocity` is a device array of
+ * coarseX*coarseY*coarseZ vec4 (ux, uy, uz, rho) -- LBM_GetVelocityBuffer of a
+ * grid of that size -- and the fine field is written on `stream` (a
+ * cudaStream_t, NULL for the legacy default stream), asynchronously.
+ * Returns LBM_OK, LBM_ERR_INVALID_ARGUMENT or LBM_ERR_CUDA. */
+int LBM_SuperResUpscale(LBMSuperRes *sr, const float *coarseVelocity, void *stream);
+/* SR_GetFineVelocityBuffer (superres.c:276-278): the device fine field,
+ * fineX*fineY*fineZ vec4, cell = x + fineX*(y + fineY*z). */
+const float *LBM_SuperResGetFineVelocity(LBMSuperRes *sr);
+/* SR_GetFineSize (superres.c:280-285). */
+void LBM_SuperResGetFineSize(LBMSuperRes *sr, int *fineX, int *fineY, int *fineZ);
+/* Copy the fine field to host memory (4 floats per fine cell) after the
+ * device is done with it; also reports a tensor-core wait that gave up
+ * (LBM_ERR_TIMEOUT).  Returns LBM_OK or an LBM_ERR_* code. */
+int LBM_SuperResCopyFine(LBMSuperRes *sr, float *host);
+
 #ifdef __cplusplus
 }
 #endif

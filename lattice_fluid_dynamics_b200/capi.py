@@ -186,6 +186,14 @@ SIGNATURES = {
     "LBM_TunnelRampFactor": (_f, [C.c_int]),
     "LBM_TunnelDefaults": (None, [_vp]),
     "LBM_TunnelRun": (C.c_int, [_vp, _vp]),
+    "LBM_SuperResCreate": (_vp, [C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p]),
+    "LBM_SuperResCreateFromArrays": (_vp, [C.c_int, C.c_int, C.c_int, _vp, C.c_longlong, _vp,
+                                           _vp]),
+    "LBM_SuperResFree": (None, [_vp]),
+    "LBM_SuperResUpscale": (C.c_int, [_vp, _vp, _vp]),
+    "LBM_SuperResGetFineVelocity": (_vp, [_vp]),
+    "LBM_SuperResGetFineSize": (None, [_vp, _vp, _vp, _vp]),
+    "LBM_SuperResCopyFine": (C.c_int, [_vp, _vp]),
 }
 
 _lib = None
@@ -716,3 +724,57 @@ class WarmNet:
         self._check(self._L.LBM_WarmNetTrainStepDevice(self._n, feat_ptr, target_ptr, batch, lr,
                                                        C.byref(loss)), "train_step_device")
         return loss.value
+
+
+class SuperRes:
+    """The velocity-field upscaler (LBM_SuperRes*): coarse vec4 field ->
+    fine field at twice the resolution, through the tensor-core MLP."""
+
+    def __init__(self, cx: int, cy: int, cz: int, weights=None, mean=None, std=None,
+                 weights_path: str | None = None, norm_path: str | None = None):
+        self._L = load()
+        self.coarse = (cx, cy, cz)
+        if weights_path is not None:
+            self._h = self._L.LBM_SuperResCreate(
+                cx, cy, cz, weights_path.encode(),
+                norm_path.encode() if norm_path is not None else None)
+        else:
+            w = np.ascontiguousarray(weights, np.float32)
+            m = np.ascontiguousarray(mean if mean is not None else np.zeros(4), np.float32)
+            sd = np.ascontiguousarray(std if std is not None else np.ones(4), np.float32)
+            self._h = self._L.LBM_SuperResCreateFromArrays(cx, cy, cz, _p(w), w.size, _p(m),
+                                                          _p(sd))
+        if not self._h:
+            raise RuntimeError("LBM_SuperResCreate failed")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.LBM_SuperResFree(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def fine_size(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        self._L.LBM_SuperResGetFineSize(self._h, C.byref(a), C.byref(b), C.byref(c))
+        return a.value, b.value, c.value
+
+    def upscale(self, coarse_device_ptr: int, stream: int = 0):
+        rc = self._L.LBM_SuperResUpscale(self._h, coarse_device_ptr, stream or None)
+        if rc != 0:
+            raise RuntimeError(f"LBM_SuperResUpscale: {rc}")
+
+    def fine(self) -> np.ndarray:
+        fx, fy, fz = self.fine_size()
+        out = np.empty((fx * fy * fz, 4), np.float32)
+        rc = self._L.LBM_SuperResCopyFine(self._h, _p(out))
+        if rc != 0:
+            raise RuntimeError(f"LBM_SuperResCopyFine: {rc}")
+        return out
+
+    def fine_device_ptr(self) -> int:
+        return self._L.LBM_SuperResGetFineVelocity(self._h) or 0

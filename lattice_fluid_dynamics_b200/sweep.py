@@ -109,7 +109,7 @@ def merge_ranks(results: list) -> dict:
 
 def run_sweep(count: int = 64, steps: int = 3000, seed: int = 1, autotune: bool = True,
               solo: bool = True, storage: str = "fp32", warmup: int = 0,
-              indices=None, tau_clamp: bool = False) -> dict:
+              indices=None, tau_clamp: bool = False, schedule: str | None = None) -> dict:
     """The sweep of `count` instances from `seed`, or of the subset
     `indices` of them (a rank's shard); per-instance results keep the
     instance's index in the full sweep."""
@@ -127,6 +127,8 @@ def run_sweep(count: int = 64, steps: int = 3000, seed: int = 1, autotune: bool 
     t0 = time.perf_counter()
     if autotune:
         batch.autotune(10)
+    if schedule is not None:  # after the autotuner's tile choice: time this schedule
+        batch.set_schedule(schedule)
     tune_s = time.perf_counter() - t0
     if warmup:
         batch.run(warmup, inlets)
@@ -189,6 +191,8 @@ def main(argv=None) -> int:
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--storage", default="fp32")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--schedule", choices=["fused", "graph"], default=None,
+                    help="run this schedule instead of the autotuner's pick")
     ap.add_argument("--no-solo", action="store_true")
     ap.add_argument("--tau-clamp", action="store_true",
                     help="viscosity through the reference driver's rule (tau >= 0.52)")
@@ -207,7 +211,7 @@ def main(argv=None) -> int:
         dims = [i["dims"] for i in geometry.sweep_instances(a.seed, a.count)]
         indices = shard(dims, world, rank)
     res = run_sweep(a.count, a.steps, a.seed, not a.no_autotune, not a.no_solo, a.storage,
-                    indices=indices, tau_clamp=a.tau_clamp)
+                    indices=indices, tau_clamp=a.tau_clamp, schedule=a.schedule)
     if world > 1:
         gathered = [None] * world
         dist.all_gather_object(gathered, res)
