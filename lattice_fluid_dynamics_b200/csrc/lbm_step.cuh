@@ -766,8 +766,8 @@ struct StepLaunch {
                 case BATCH_SET_REG_SMAG: k_step_batch_pair<S, BATCH_SET_REG_SMAG><<<tiles, blk, 0, s>>>(p); break;
                 case BATCH_SET_MRT: k_step_batch_pair<S, BATCH_SET_MRT><<<tiles, blk, 0, s>>>(p); break;
                 case BATCH_SET_MRT_SMAG: k_step_batch_pair<S, BATCH_SET_MRT_SMAG><<<tiles, blk, 0, s>>>(p); break;
-                case BATCH_SET_BGK_REG: k_step_batch_pair<S, BATCH_SET_BGK_REG><<<tiles, blk, 0, s>>>(p); break;
-                default: k_step_batch_pair<S, BATCH_SET_ALL><<<tiles, blk, 0, s>>>(p); break;
+                // a launch group holds one operator (lbm_batch.cu, make_groups)
+                default: return cudaErrorInvalidValue;
             }
             return cudaGetLastError();
         } else {
@@ -788,8 +788,8 @@ struct StepLaunch {
             case BATCH_SET_REG_SMAG: k_step_batch<S, BATCH_SET_REG_SMAG><<<tiles, 256, 0, s>>>(p); break;
             case BATCH_SET_MRT: k_step_batch<S, BATCH_SET_MRT><<<tiles, 256, 0, s>>>(p); break;
             case BATCH_SET_MRT_SMAG: k_step_batch<S, BATCH_SET_MRT_SMAG><<<tiles, 256, 0, s>>>(p); break;
-            case BATCH_SET_BGK_REG: k_step_batch<S, BATCH_SET_BGK_REG><<<tiles, 256, 0, s>>>(p); break;
-            default: k_step_batch<S, BATCH_SET_ALL><<<tiles, 256, 0, s>>>(p); break;
+            // a launch group holds one operator (lbm_batch.cu, make_groups)
+            default: return cudaErrorInvalidValue;
         }
         return cudaGetLastError();
     }

@@ -474,12 +474,15 @@ __host__ __device__ constexpr int pair_minb() {
     return SMAG ? 6 : 7;
 #endif
 }
+// Batched launches read each grid's arguments from shared memory and hold
+// more registers; they are capped at 96 (5 blocks per SM) unless
+// LBM_PAIR_MINB_BATCH says otherwise (measurements).
 __host__ __device__ constexpr int pair_minb_set(int set) {
-    return set == BATCH_SET_BGK ? pair_minb<OP_BGK, false>()
-         : set == BATCH_SET_REG ? pair_minb<OP_REG, false>()
-         : set == BATCH_SET_MRT ? pair_minb<OP_MRT, false>()
-         : set == BATCH_SET_MRT_SMAG ? pair_minb<OP_MRT, true>()
-         : 6;
+#ifdef LBM_PAIR_MINB_BATCH
+    return (void)set, LBM_PAIR_MINB_BATCH;
+#else
+    return (void)set, 5;
+#endif
 }
 
 // Where the scalar fallback parks the second cell of a pair (one array per
