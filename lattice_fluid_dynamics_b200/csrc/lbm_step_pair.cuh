@@ -501,63 +501,81 @@ __device__ __forceinline__ void pair_load(const void *base, unsigned cell, int i
     }
 }
 
-// One thread: the cells (x0, y, z) and (x0 + 1, y, z), x0 even.  FUSED:
-// pull-stream (+ Bouzidi) then collide; otherwise collide the buffer's own
-// values (the first step after initialisation).
-template <class S, int OP, bool SMAG, bool FUSED>
-__device__ __forceinline__ void step_pair(const StepArgs &a, const PairTable &t, int x0, int y,
-                                          int z) {
+// The pull of one pair in an interior row (y and z away from the grid
+// faces) at warp-uniform offsets.  The inlet / outlet pairs of the row take
+// the reference's x-edge rule by a per-lane pointer select: a cell whose
+// source x lies outside the grid keeps its own value (lbm_stream.comp:
+// 116-127).  Calls copy(i, lane-x source, lane-y source, aligned pair).
+template <class S, class Copy>
+__device__ __forceinline__ void pair_pull_interior(const StepArgs &a, const PairTable &t,
+                                                   int x0, unsigned cell0, Copy copy) {
     using T = typename S::T;
-    if (x0 >= a.nx || y >= a.ny) return;
-    const unsigned cell0 = (unsigned)x0 + (unsigned)a.nx * ((unsigned)y + (unsigned)a.ny * z);
-    const uchar2 fl = *reinterpret_cast<const uchar2 *>(a.flags + cell0);
-    const uint8_t flagA = fl.x, flagB = fl.y;
-    float fa[19], fb[19];
-    // A warp covers one row, so this test is uniform across the warp.
-    const bool interior_row = y > 0 && y + 1 < a.ny && z > 0 && z + 1 < a.nz;
-    if (FUSED) {
-        if (interior_row) {
-            // Pull at warp-uniform offsets.  The inlet / outlet pairs of the
-            // row take the reference's x-edge rule by a per-lane pointer
-            // select: a cell whose source x lies outside the grid keeps its
-            // own value (lbm_stream.comp:116-127).
-            const bool edgeA = x0 == 0, edgeB = x0 + 2 == a.nx;
+    const bool edgeA = x0 == 0, edgeB = x0 + 2 == a.nx;
 #pragma unroll
-            for (int i = 0; i < 19; i++) {
-                if (cx(i) == 0) {
-                    pair_load<S>(t.pull[i], cell0, i, fa[i], fb[i], true);
+    for (int i = 0; i < 19; i++) {
+        const T *pull = static_cast<const T *>(t.pull[i]) + cell0;
+        if (cx(i) == 0) {
+            copy(i, pull, pull + 1, true);
+        } else {
+            const T *own = static_cast<const T *>(t.own[i]) + cell0;
+            const bool keepA = cx(i) == 1 && edgeA, keepB = cx(i) == -1 && edgeB;
+            copy(i, keepA ? own : pull, keepB ? own + 1 : pull + 1, false);
+        }
+    }
+}
+
+// The populations of one pair before Bouzidi: FUSED, the pull (interior
+// row or, on a y / z face row, the wrap / clamp rules of gather_pull);
+// otherwise the buffer's own values (the first step after initialisation).
+template <class S, bool FUSED>
+__device__ __forceinline__ void pair_gather(const StepArgs &a, const PairTable &t, int x0, int y,
+                                            int z, unsigned cell0, float (&fa)[19],
+                                            float (&fb)[19]) {
+    using T = typename S::T;
+    if (FUSED) {
+        // a warp covers one row, so this test is uniform across the warp
+        if (y > 0 && y + 1 < a.ny && z > 0 && z + 1 < a.nz) {
+            pair_pull_interior<S>(a, t, x0, cell0, [&](int i, const T *pa, const T *pb, bool al) {
+                if (al) {
+                    S::load2(pa, i, fa[i], fb[i]);
                 } else {
-                    const T *pull = static_cast<const T *>(t.pull[i]) + cell0;
-                    const T *own = static_cast<const T *>(t.own[i]) + cell0;
-                    const bool keepA = cx(i) == 1 && edgeA, keepB = cx(i) == -1 && edgeB;
-                    fa[i] = S::load(keepA ? own : pull, i);
-                    fb[i] = S::load(keepB ? own + 1 : pull + 1, i);
+                    fa[i] = S::load(pa, i);
+                    fb[i] = S::load(pb, i);
                 }
-            }
+            });
         } else {
             const Rows rw = neighbour_rows(a, y, z);
             const T *src = static_cast<const T *>(a.src);
             gather_pull<S>(a, src, x0, rw, (long long)cell0, fa);
             gather_pull<S>(a, src, x0 + 1, rw, (long long)cell0 + 1, fb);
         }
-        if ((flagA | flagB) & FLAG_BOUNDARY) {
-            const Rows rw = neighbour_rows(a, y, z);
-            const T *src = static_cast<const T *>(a.src);
-            if (flagA & FLAG_BOUNDARY) bouzidi<S>(a, src, x0, rw, (long long)cell0, fa);
-            if (flagB & FLAG_BOUNDARY) bouzidi<S>(a, src, x0 + 1, rw, (long long)cell0 + 1, fb);
-        }
     } else {
 #pragma unroll
         for (int i = 0; i < 19; i++) pair_load<S>(t.own[i], cell0, i, fa[i], fb[i], true);
     }
+}
 
+// Bouzidi on the pair's link-owning cells (FUSED), the collision and the
+// store of one pair; returns the pair's guard resets.
+template <class S, int OP, bool SMAG, bool FUSED>
+__device__ __forceinline__ int pair_finish(const StepArgs &a, const PairTable &t, int x0, int y,
+                                           int z, unsigned cell0, uint8_t flagA, uint8_t flagB,
+                                           float (&fa)[19], float (&fb)[19]) {
+    using T = typename S::T;
+    if (FUSED && ((flagA | flagB) & FLAG_BOUNDARY)) {
+        const Rows rw = neighbour_rows(a, y, z);
+        const T *src = static_cast<const T *>(a.src);
+        if (flagA & FLAG_BOUNDARY) bouzidi<S>(a, src, x0, rw, (long long)cell0, fa);
+        if (flagB & FLAG_BOUNDARY) bouzidi<S>(a, src, x0 + 1, rw, (long long)cell0 + 1, fb);
+    }
     int resets = 0;
     const int solidA = flagA & FLAG_SOLID_MASK, solidB = flagB & FLAG_SOLID_MASK;
-    // The scalar per-cell code for both cells of the pair, one after the
-    // other (one code instance).  The second cell's populations wait in
-    // shared memory meanwhile (stride PAIR_THREADS: conflict-free), so this
-    // rare path does not raise the kernel's register demand.
-    auto scalar_pair = [&]() {
+    if (solidA == 1 || solidB == 1) {
+        // A body cell in the pair: the scalar per-cell code for both cells,
+        // one after the other (one code instance).  The second cell's
+        // populations wait in shared memory meanwhile (stride PAIR_THREADS:
+        // conflict-free), so this rare path does not raise the kernel's
+        // register demand.
         float *park = pair_park;
         const int slot = threadIdx.x + blockDim.x * threadIdx.y;
 #pragma unroll
@@ -575,23 +593,21 @@ __device__ __forceinline__ void step_pair(const StepArgs &a, const PairTable &t,
             for (int i = 0; i < 19; i++)
                 S::store(static_cast<T *>(t.dst[i]) + cell0 + c, fn[i], i);
         }
-    };
-    auto store_pair = [&](const P (&fn)[19]) {
-#pragma unroll
-        for (int i = 0; i < 19; i++)
-            S::store2(static_cast<T *>(t.dst[i]) + cell0, fn[i].x, fn[i].y, i);
-    };
-    if (solidA == 1 || solidB == 1) {
-        // a body cell in the pair
-        scalar_pair();
     } else {
         P fn[19];
         bool resetA, resetB;
         pair_collide_fluid<OP, SMAG>(fa, fb, x0 == 0, x0 + 1 == a.nx - 1, a.inX, a.inY, a.inZ,
                                      a.tau, a.omega, a.smag18, t.nz, fn, resetA, resetB);
         resets = (int)resetA + (int)resetB;
-        store_pair(fn);
+#pragma unroll
+        for (int i = 0; i < 19; i++)
+            S::store2(static_cast<T *>(t.dst[i]) + cell0, fn[i].x, fn[i].y, i);
     }
+    return resets;
+}
+
+// guard resets of the warp added to the grid's counter (one atomic)
+__device__ __forceinline__ void pair_count_resets(const StepArgs &a, int resets) {
     const unsigned active = __activemask();
     const unsigned any = __ballot_sync(active, resets > 0);
     if (any) {
@@ -600,6 +616,21 @@ __device__ __forceinline__ void step_pair(const StepArgs &a, const PairTable &t,
         const unsigned lane = (threadIdx.x + blockDim.x * threadIdx.y) & 31u;
         if (lane == (unsigned)(__ffs(active) - 1) && v) atomicAdd(a.guard, (unsigned long long)v);
     }
+}
+
+// One thread: the cells (x0, y, z) and (x0 + 1, y, z), x0 even.  FUSED:
+// pull-stream (+ Bouzidi) then collide; otherwise collide the buffer's own
+// values (the first step after initialisation).
+template <class S, int OP, bool SMAG, bool FUSED>
+__device__ __forceinline__ void step_pair(const StepArgs &a, const PairTable &t, int x0, int y,
+                                          int z) {
+    if (x0 >= a.nx || y >= a.ny) return;
+    const unsigned cell0 = (unsigned)x0 + (unsigned)a.nx * ((unsigned)y + (unsigned)a.ny * z);
+    const uchar2 fl = *reinterpret_cast<const uchar2 *>(a.flags + cell0);
+    float fa[19], fb[19];
+    pair_gather<S, FUSED>(a, t, x0, y, z, cell0, fa, fb);
+    const int resets = pair_finish<S, OP, SMAG, FUSED>(a, t, x0, y, z, cell0, fl.x, fl.y, fa, fb);
+    pair_count_resets(a, resets);
 }
 
 // Blocks of PAIR_THREADS threads, blockDim.x along x (two cells each) and
