@@ -496,20 +496,27 @@ def main(argv=None) -> int:
     return 0
 
 
-def _train_from_snapshots(net, a, half, res):
+def train_from_snapshots(net, count: int, val: int, seed: int, snapshot_dims, snapshot_steps: int,
+                         epochs: int, batch: int, lr: float, res: dict | None = None):
+    """Solve `count + val` random shapes (seed) from uniform flow at
+    snapshot_dims for snapshot_steps, keep those that never tripped the
+    stability guard, set the network's output scaling from the targets'
+    spread, and train on the first share with the rest as validation.
+    Returns the loss history; `res` (if given) receives the bookkeeping."""
+    import torch
+    res = {} if res is None else res
     t0 = time.perf_counter()
-    feats, tgts, resets = make_dataset(a.train + a.val, a.seed, half, a.snapshot_steps)
+    feats, tgts, resets = make_dataset(count + val, seed, snapshot_dims, snapshot_steps)
     res["dataset_s"] = time.perf_counter() - t0
     res["dataset_unstable"] = int((resets > 0).sum())
     res["dataset_unstable_shapes"] = [
-        {k: v for k, v in random_union(a.seed, int(i)).items() if k in ("index", "U", "Re",
-                                                                      "length_world")}
+        {k: v for k, v in random_union(seed, int(i)).items() if k in ("index", "U", "Re",
+                                                                    "length_world")}
         for i in np.nonzero(resets > 0)[0][:20]]
     keep = np.nonzero(resets == 0)[0]
-    import torch
     kt = torch.from_numpy(keep).cuda()
     feats, tgts = feats.index_select(0, kt), tgts.index_select(0, kt)
-    ntr = int(round(len(keep) * a.train / (a.train + a.val)))
+    ntr = int(round(len(keep) * count / (count + val)))
     t = tgts.reshape(-1, 4)
     res["target_stats"] = {"mean": t.mean(0).tolist(), "std": t.std(0).tolist(),
                            "min": t.min(0).values.tolist(), "max": t.max(0).values.tolist()}
@@ -518,11 +525,17 @@ def _train_from_snapshots(net, a, half, res):
     tgts = ((tgts - mean) / std).clamp(-8.0, 8.0)  # rare stagnation-point outliers
     net.set_output_scaling(std.cpu().numpy(), mean.cpu().numpy())
     res["output_scaling"] = {"scale": std.tolist(), "shift": mean.tolist()}
-    hist, tsec = train(net, feats[:ntr], tgts[:ntr], a.epochs, a.batch, a.lr,
-                       val=(feats[ntr:], tgts[ntr:]))
+    hist, tsec = train(net, feats[:ntr], tgts[:ntr], epochs, batch, lr,
+                       val=(feats[ntr:], tgts[ntr:]) if ntr < len(keep) else None)
     res["train_s"] = tsec
     res["history"] = hist
+    res["trained_on"] = ntr
     return hist
+
+
+def _train_from_snapshots(net, a, half, res):
+    return train_from_snapshots(net, a.train, a.val, a.seed, half, a.snapshot_steps, a.epochs,
+                                a.batch, a.lr, res)
 
 
 if __name__ == "__main__":
