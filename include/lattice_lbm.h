@@ -381,6 +381,14 @@ int LBM_NNConvWeightGrad(const void *x, int xStride, int xOff, int cin, const vo
  * waiting for its tensor-core work since the last call, else LBM_OK. */
 int LBM_NNTakeError(void);
 
+/* Which forward / input-gradient kernel LBM_NNConvForward and the network
+ * use: 0 (default) the halo-tiled kernel wherever the shape allows it (input
+ * channels a multiple of 16, NX a multiple of 8, NY a multiple of 16,
+ * coutPad 16 / 32 / 48 / 64 / 96) and the im2col-gather kernel elsewhere;
+ * 1 the gather kernel for every shape.  Process-wide; not thread-safe
+ * against concurrent launches.  LBM_OK or LBM_ERR_INVALID_ARGUMENT. */
+int LBM_NNSetConvPath(int path);
+
 /* The warm-start network: a 4-level 3D conv encoder-decoder (8->16->32->64
  * ->128 channels and back, skip connections, ~1.9 M parameters, leaky ReLU)
  * mapping per-voxel (solid fraction, U, Re) at 1/4 of the grid's resolution

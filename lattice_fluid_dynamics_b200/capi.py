@@ -162,6 +162,7 @@ SIGNATURES = {
                                        C.c_int, _vp, C.c_int, _vp, C.c_longlong, C.c_int,
                                        C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
     "LBM_NNTakeError": (C.c_int, []),
+    "LBM_NNSetConvPath": (C.c_int, [C.c_int]),
     "LBM_WarmNetParamCount": (C.c_longlong, []),
     "LBM_WarmNetCreate": (_vp, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint]),
     "LBM_WarmNetFree": (None, [_vp]),

@@ -4,11 +4,14 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <map>
 #include <mutex>
+#include <utility>
 
 #include "lbm_internal.h"
 #include "lbm_nn.h"
 #include "lbm_nn_gemm.cuh"
+#include "lbm_nn_halo.cuh"
 
 namespace lbm {
 namespace nn {
@@ -50,12 +53,148 @@ int *err_ptr() {
     return p;
 }
 
+// Epilogue of a split forward convolution: the partial sums of each output
+// (voxel, 8 columns) added over the splits in order, then fwd_store.
+__global__ void k_conv_fwd_finish(const ConvFwdArgs a, int nt, int splits) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int groups = a.cout_store >> 3;
+    if (i >= a.m * groups) return;
+    const long long m = i / groups;
+    const int col = (int)(i - m * groups) * 8;
+    float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int p = 0; p < splits; p++) {
+        const float4 *q =
+            reinterpret_cast<const float4 *>(a.partial + ((long long)p * a.m + m) * nt + col);
+        const float4 x = q[0], y = q[1];
+        v[0] += x.x; v[1] += x.y; v[2] += x.z; v[3] += x.w;
+        v[4] += y.x; v[5] += y.y; v[6] += y.z; v[7] += y.w;
+    }
+    fwd_store(a, m, col, v);
+}
+
+// FP32 workspace of split forward convolutions, one per stream (calls on
+// one stream are ordered; calls on different streams do not share), grown
+// on demand and kept.
+float *split_workspace(cudaStream_t s, size_t bytes) {
+    static std::mutex lock;
+    static std::map<cudaStream_t, std::pair<void *, size_t>> bufs;
+    std::lock_guard<std::mutex> guard(lock);
+    auto &b = bufs[s];
+    if (b.second < bytes) {
+        if (b.first) {
+            if (cudaStreamSynchronize(s) != cudaSuccess) return nullptr;
+            cudaFree(b.first);
+            b = {nullptr, 0};
+        }
+        void *p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+        b = {p, bytes};
+    }
+    return static_cast<float *>(b.first);
+}
+
 template <int NT>
 cudaError_t fwd_nt(ConvFwdArgs a, int slot, cudaStream_t s) {
     cudaError_t e = set_attr<NT>(slot);
     if (e != cudaSuccess) return e;
     const unsigned blocks = (unsigned)((a.m + 127) / 128);
+    const int nchunks = a.k_pad / KC;
+    // Few row tiles and a long reduction: split the reduction over CTAs so
+    // that about two CTAs per SM work, at least 4 slices each, and sum the
+    // FP32 partials in a second kernel (not inside a stream capture).
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (blocks < 148 && nchunks >= 8 && cudaStreamIsCapturing(s, &cap) == cudaSuccess &&
+        cap == cudaStreamCaptureStatusNone) {
+        int splits = (int)((296 + blocks - 1) / blocks);
+        if (splits > nchunks / 4) splits = nchunks / 4;
+        const int cps = (nchunks + splits - 1) / splits;
+        splits = (nchunks + cps - 1) / cps;
+        float *ws = splits > 1 ? split_workspace(s, (size_t)splits * a.m * NT * sizeof(float))
+                               : nullptr;
+        if (ws) {
+            a.partial = ws;
+            a.chunks_per_split = cps;
+            k_conv_fwd<NT><<<dim3(blocks, (unsigned)splits), 128, gemm_smem_bytes<NT>(), s>>>(a);
+            const long long outs = a.m * (a.cout_store / 8);
+            k_conv_fwd_finish<<<(unsigned)((outs + 255) / 256), 256, 0, s>>>(a, NT, splits);
+            return cudaGetLastError();
+        }
+    }
+    a.partial = nullptr;
     k_conv_fwd<NT><<<blocks, 128, gemm_smem_bytes<NT>(), s>>>(a);
+    return cudaGetLastError();
+}
+
+// 0: the halo-tiled forward kernel where a convolution's shape allows it;
+// 1: the gather kernel for every shape (LBM_NNSetConvPath, for comparisons)
+int g_conv_path = 0;
+
+bool halo_shape_ok(const ConvFwdArgs &a, int nt) {
+    return g_conv_path == 0 && a.cin % 16 == 0 && a.x_stride % 8 == 0 && a.x_off % 8 == 0 &&
+           a.d.nx % 8 == 0 && a.d.ny % 16 == 0 &&
+           (nt == 16 || nt == 32 || nt == 48 || nt == 64 || nt == 96) &&
+           (long long)a.d.nb * a.d.nz * (a.d.ny / 16) * (a.d.nx / 8) < (1ll << 31);
+}
+
+template <int NT>
+cudaError_t fwd_halo_nt(ConvFwdArgs a, cudaStream_t s) {
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    static int per_sm = 0, sms = 0;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_conv_fwd_halo<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    halo_smem_bytes<NT>());
+        int dev = 0;
+        if (attr == cudaSuccess) attr = cudaGetDevice(&dev);
+        if (attr == cudaSuccess)
+            attr = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (attr == cudaSuccess)
+            attr = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv_fwd_halo<NT>, 128,
+                                                                 halo_smem_bytes<NT>());
+        if (attr == cudaSuccess && per_sm < 1) attr = cudaErrorInvalidConfiguration;
+    });
+    if (attr != cudaSuccess) return attr;
+    const long long tiles = (long long)a.d.nb * a.d.nz * (a.d.ny / 16) * (a.d.nx / 8);
+    const long long cap = (long long)per_sm * sms;
+    const unsigned blocks = (unsigned)(tiles < cap ? tiles : cap);
+    k_conv_fwd_halo<NT><<<blocks, 128, halo_smem_bytes<NT>(), s>>>(a, (int)tiles);
+    return cudaGetLastError();
+}
+
+bool wgrad_halo_ok(const ConvWgradArgs &a, int nt) {
+    return g_conv_path == 0 && a.cin % 16 == 0 && a.x_stride % 8 == 0 && a.x_off % 8 == 0 &&
+           a.g_stride % 8 == 0 && a.g_stride >= nt && a.d.nx % 8 == 0 && a.d.ny % 16 == 0 &&
+           (nt == 16 || nt == 32 || nt == 64 || nt == 128) &&
+           (long long)a.d.nb * a.d.nz * (a.d.ny / 16) * (a.d.nx / 8) < (1ll << 31);
+}
+
+// Runs k_conv_wgrad_halo with at most `splits` tile ranges (the partial
+// workspace holds that many); returns the number used in *used.
+template <int NT>
+cudaError_t wgrad_halo_nt(ConvWgradArgs a, unsigned splits, unsigned *used, cudaStream_t s) {
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    static int sms = 0;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_conv_wgrad_halo<NT>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, WG_SMEM_BYTES);
+        int dev = 0;
+        if (attr == cudaSuccess) attr = cudaGetDevice(&dev);
+        if (attr == cudaSuccess)
+            attr = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    });
+    if (attr != cudaSuccess) return attr;
+    const long long tiles = (long long)a.d.nb * a.d.nz * (a.d.ny / 16) * (a.d.nx / 8);
+    const int slices = a.cin / 16;
+    long long sp = (sms + slices - 1) / slices;  // one CTA per SM (512 TMEM columns each)
+    if (sp > (long long)splits) sp = splits;
+    if (sp > tiles) sp = tiles;
+    if (sp < 1) sp = 1;
+    const long long per = (tiles + sp - 1) / sp;
+    sp = (tiles + per - 1) / per;
+    k_conv_wgrad_halo<NT><<<dim3(slices, (unsigned)sp), 128, WG_SMEM_BYTES, s>>>(a, (int)tiles,
+                                                                                 (int)per);
+    *used = (unsigned)sp;
     return cudaGetLastError();
 }
 
@@ -68,15 +207,18 @@ cudaError_t wgrad_nt(ConvWgradArgs a, int slot, unsigned splits, cudaStream_t s)
     return cudaGetLastError();
 }
 
+
 // dW[n][k] = sum over splits of partial[split][k][n], n < cout, k < k_real
+// (thread i = k * cout + n: a warp reads contiguous partials)
 __global__ void k_wgrad_reduce(const float *__restrict__ partial, int splits, int k_pad, int nt,
                                int cout, int k_real, float *__restrict__ dw, int accumulate) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= cout * k_real) return;
-    const int n = i / k_real, k = i - n * k_real;
+    const int k = i / cout, n = i - k * cout;
     float s = 0.f;
     for (int p = 0; p < splits; p++) s += partial[((long long)p * k_pad + k) * nt + n];
-    dw[i] = accumulate ? dw[i] + s : s;
+    float *o = dw + (long long)n * k_real + k;
+    *o = accumulate ? *o + s : s;
 }
 
 // Wt[ci][(26 - tap) * cout + co] = W[co][tap * cin + ci]  (flip and transpose)
@@ -100,6 +242,15 @@ cudaError_t conv_forward(const ConvFwdArgs &a0, int nt, cudaStream_t s) {
     ConvFwdArgs a = a0;
     a.err = err_ptr();
     if (!a.err) return cudaErrorInvalidDevicePointer;
+    if (halo_shape_ok(a, nt)) {
+        switch (nt) {
+            case 16: return fwd_halo_nt<16>(a, s);
+            case 32: return fwd_halo_nt<32>(a, s);
+            case 48: return fwd_halo_nt<48>(a, s);
+            case 64: return fwd_halo_nt<64>(a, s);
+            default: return fwd_halo_nt<96>(a, s);
+        }
+    }
     switch (nt) {
         case 16: return fwd_nt<16>(a, 0, s);
         case 32: return fwd_nt<32>(a, 1, s);
@@ -118,12 +269,23 @@ cudaError_t conv_wgrad(const ConvWgradArgs &a0, int nt, unsigned splits, float *
     a.err = err_ptr();
     if (!a.err) return cudaErrorInvalidDevicePointer;
     cudaError_t e;
-    switch (nt) {
-        case 16: e = wgrad_nt<16>(a, 0, splits, s); break;
-        case 32: e = wgrad_nt<32>(a, 1, splits, s); break;
-        case 64: e = wgrad_nt<64>(a, 3, splits, s); break;
-        case 128: e = wgrad_nt<128>(a, 5, splits, s); break;
-        default: return cudaErrorInvalidValue;
+    if (wgrad_halo_ok(a, nt)) {
+        unsigned used = splits;
+        switch (nt) {
+            case 16: e = wgrad_halo_nt<16>(a, splits, &used, s); break;
+            case 32: e = wgrad_halo_nt<32>(a, splits, &used, s); break;
+            case 64: e = wgrad_halo_nt<64>(a, splits, &used, s); break;
+            default: e = wgrad_halo_nt<128>(a, splits, &used, s); break;
+        }
+        splits = used;
+    } else {
+        switch (nt) {
+            case 16: e = wgrad_nt<16>(a, 0, splits, s); break;
+            case 32: e = wgrad_nt<32>(a, 1, splits, s); break;
+            case 64: e = wgrad_nt<64>(a, 3, splits, s); break;
+            case 128: e = wgrad_nt<128>(a, 5, splits, s); break;
+            default: return cudaErrorInvalidValue;
+        }
     }
     if (e != cudaSuccess) return e;
     const int rows = cout_write > 0 ? cout_write : a.cout;
@@ -241,5 +403,11 @@ int LBM_NNConvWeightGrad(const void *x, int xStride, int xOff, int cin, const vo
 }
 
 int LBM_NNTakeError(void) { return take_error() ? LBM_ERR_TIMEOUT : LBM_OK; }
+
+int LBM_NNSetConvPath(int path) {
+    if (path != 0 && path != 1) return LBM_ERR_INVALID_ARGUMENT;
+    g_conv_path = path;
+    return LBM_OK;
+}
 
 }  // extern "C"

@@ -78,6 +78,10 @@ struct ConvFwdArgs {
     Dims d;
     long long m;             // voxels
     int *err;
+    // split reduction: CTA (x, y) sums reduction slices [y cps, (y + 1) cps)
+    // into partial[y][m][nt] (FP32); k_conv_fwd_finish applies the epilogue
+    float *partial;          // null: no split
+    int chunks_per_split;
 };
 
 struct ConvWgradArgs {
@@ -196,6 +200,31 @@ __device__ __forceinline__ void gemm_tile(int nchunks, int *err, Load load, Epi 
 
 __device__ __forceinline__ float leaky(float v) { return v > 0.f ? v : 0.1f * v; }
 
+// Epilogue of the forward convolution for 8 accumulator columns of output
+// voxel m: bias, activation, BF16 and / or FP32 store.
+__device__ __forceinline__ void fwd_store(const ConvFwdArgs &a, long long m, int col,
+                                          const float (&v)[8]) {
+    if (m >= a.m || col >= a.cout_store) return;
+    float o[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        float t = v[i] + (a.bias ? a.bias[col + i] : 0.f);
+        o[i] = a.act == 1 ? leaky(t) : t;
+    }
+    if (a.y) {
+        __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) h[i] = __float2bfloat16_rn(o[i]);
+        *reinterpret_cast<uint4 *>(a.y + m * a.y_stride + a.y_off + col) =
+            *reinterpret_cast<const uint4 *>(h);
+    }
+    if (a.y32) {
+        float *p = a.y32 + m * a.y_stride + a.y_off + col;
+#pragma unroll
+        for (int i = 0; i < 8; i++) p[i] = a.accumulate ? p[i] + o[i] : o[i];
+    }
+}
+
 // Forward convolution (also the input gradient, run on the flipped,
 // transposed weights with act = 0).
 template <int NT>
@@ -211,8 +240,12 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const ConvFwdArgs a) {
         rv[i] = m < a.m;
         voxel_coords(a.d, rv[i] ? m : 0, rb[i], rz[i], ry[i], rx[i]);
     }
-    const int nchunks = a.k_pad / KC;
-    auto load = [&](int c, uint8_t *as, uint8_t *bs) {
+    const int all_chunks = a.k_pad / KC;
+    const int c0 = a.partial ? (int)blockIdx.y * a.chunks_per_split : 0;
+    const int nchunks =
+        a.partial ? max(0, min(all_chunks, c0 + a.chunks_per_split) - c0) : all_chunks;
+    auto load = [&](int cl, uint8_t *as, uint8_t *bs) {
+        const int c = c0 + cl;
         const int kc = tid & 7;
         const int k = c * KC + kc * 8;
         int tap = 0, cin = 0;
@@ -240,25 +273,13 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const ConvFwdArgs a) {
         }
     };
     auto epi = [&](int row, int col, const float (&v)[8]) {
-        const long long m = m0 + row;
-        if (m >= a.m || col >= a.cout_store) return;
-        float o[8];
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            float t = v[i] + (a.bias ? a.bias[col + i] : 0.f);
-            o[i] = a.act == 1 ? leaky(t) : t;
-        }
-        if (a.y) {
-            __align__(16) __nv_bfloat16 h[8];
-#pragma unroll
-            for (int i = 0; i < 8; i++) h[i] = __float2bfloat16_rn(o[i]);
-            *reinterpret_cast<uint4 *>(a.y + m * a.y_stride + a.y_off + col) =
-                *reinterpret_cast<const uint4 *>(h);
-        }
-        if (a.y32) {
-            float *p = a.y32 + m * a.y_stride + a.y_off + col;
-#pragma unroll
-            for (int i = 0; i < 8; i++) p[i] = a.accumulate ? p[i] + o[i] : o[i];
+        if (!a.partial) {
+            fwd_store(a, m0 + row, col, v);
+        } else if (m0 + row < a.m) {
+            float4 *p = reinterpret_cast<float4 *>(
+                a.partial + ((long long)blockIdx.y * a.m + m0 + row) * NT + col);
+            p[0] = make_float4(v[0], v[1], v[2], v[3]);
+            p[1] = make_float4(v[4], v[5], v[6], v[7]);
         }
     };
     gemm_tile<NT>(nchunks, a.err, load, epi);

@@ -161,40 +161,79 @@ __global__ void k_act_bwd(const float *__restrict__ dout, int ds, int dof,
 }
 
 // loss and its gradient on the 4 output channels (prediction stride 16)
+// Loss gradient of every output channel (16 per voxel, 4 real) and the
+// squared error summed into *loss: a grid-stride loop, one FP64 atomic per
+// block.
 __global__ void k_loss(const __nv_bfloat16 *__restrict__ pred, const float *__restrict__ target,
                        long long m, float scale, __nv_bfloat16 *__restrict__ g,
                        double *__restrict__ loss) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double local = 0.0;
-    if (i < m * 16) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m * 16;
+         i += (long long)gridDim.x * blockDim.x) {
         const int ch = (int)(i & 15);
         const long long v = i >> 4;
         float r = 0.f;
         if (ch < 4) {
             const float d = __bfloat162float(pred[i]) - target[4 * v + ch];
-            local = (double)d * d;
+            local += (double)d * d;
             r = scale * d;
         }
         g[i] = __float2bfloat16_rn(r);
     }
     for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
-    if ((threadIdx.x & 31) == 0 && local != 0.0) atomicAdd(loss, local);
+    __shared__ double part[8];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = local;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += part[w];
+        if (t != 0.0) atomicAdd(loss, t);
+    }
 }
 
-// db[c] = sum over voxels of g[v][c] (fixed order per channel)
-__global__ void k_bias_grad(const __nv_bfloat16 *__restrict__ g, int nt, long long m,
-                            float *__restrict__ db) {
-    const int c = blockIdx.x;
-    double acc = 0.0;
-    for (long long v = threadIdx.x; v < m; v += blockDim.x) acc += __bfloat162float(g[v * nt + c]);
-    __shared__ double part[256];
-    part[threadIdx.x] = acc;
-    __syncthreads();
-    for (int s = 128; s > 0; s >>= 1) {
-        if ((int)threadIdx.x < s) part[threadIdx.x] += part[threadIdx.x + s];
-        __syncthreads();
+// Bias gradient, pass 1: block b sums rows [b * BG_ROWS, (b + 1) * BG_ROWS)
+// of g (nt channels per row, 8 per thread and 16-byte load) per channel in
+// FP32 and writes partial[b][nt].
+constexpr int BG_ROWS = 512;
+__global__ void k_bias_grad_part(const __nv_bfloat16 *__restrict__ g, int nt, long long m,
+                                 float *__restrict__ partial) {
+    const int groups = nt >> 3;             // 16-byte groups per row
+    const int rows_per_pass = 256 / groups;  // nt <= 256
+    const int grp = threadIdx.x % groups, r0 = threadIdx.x / groups;
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const long long base = (long long)blockIdx.x * BG_ROWS;
+    if (r0 < rows_per_pass) {
+        for (int r = r0; r < BG_ROWS; r += rows_per_pass) {
+            const long long v = base + r;
+            if (v >= m) break;
+            const uint4 q = *reinterpret_cast<const uint4 *>(g + v * nt + grp * 8);
+            const __nv_bfloat16 *h = reinterpret_cast<const __nv_bfloat16 *>(&q);
+#pragma unroll
+            for (int i = 0; i < 8; i++) acc[i] += __bfloat162float(h[i]);
+        }
     }
-    if (threadIdx.x == 0) db[c] = (float)part[0];
+    __shared__ float red[256][9];
+#pragma unroll
+    for (int i = 0; i < 8; i++) red[threadIdx.x][i] = acc[i];
+    __syncthreads();
+    // thread c < nt sums channel c over the passes in a fixed order
+    if ((int)threadIdx.x < nt) {
+        const int c = threadIdx.x, cg = c >> 3, ci = c & 7;
+        float t = 0.f;
+        for (int r = 0; r < rows_per_pass; r++) t += red[r * groups + cg][ci];
+        partial[(long long)blockIdx.x * nt + c] = t;
+    }
+}
+
+// Bias gradient, pass 2: db[c] = sum over blocks of partial[b][c] (FP64,
+// fixed order).
+__global__ void k_bias_grad_sum(const float *__restrict__ partial, int blocks, int nt, int cout,
+                                float *__restrict__ db) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cout) return;
+    double t = 0.0;
+    for (int b = 0; b < blocks; b++) t += partial[(long long)b * nt + c];
+    db[c] = (float)t;
 }
 
 // sum of squares of the gradient (for global-norm clipping)
@@ -411,6 +450,7 @@ struct LBMWarmNet {
     long long ws_bytes = 0;
     float *feat = nullptr, *target = nullptr, *pred32 = nullptr;
     double *loss = nullptr;
+    float *bias_part = nullptr;  // per-block partial bias gradients
     int error = 0;
     OutScale out_scale = {{1.f, 1.f, 1.f, 1.f}, {0.f, 0.f, 0.f, 0.f}};
     float clip = 0.f;
@@ -592,8 +632,8 @@ bool backward(LBMWarmNet *n, const float *target_dev, int nb) {
     cudaStream_t s = n->stream;
     const long long m1 = n->m(0, nb);
     if (!ok(n, cudaMemsetAsync(n->loss, 0, sizeof(double), s))) return false;
-    k_loss<<<nblk(m1 * 16), 256, 0, s>>>(n->pred, target_dev, m1, 2.0f / (float)(m1 * 4), n->g,
-                                         n->loss);
+    k_loss<<<148 * 8, 256, 0, s>>>(n->pred, target_dev, m1, 2.0f / (float)(m1 * 4), n->g,
+                                   n->loss);
     if (!ok(n, cudaGetLastError())) return false;
     for (int l = NLAYERS - 1; l >= 0; l--) {
         const int lv = kLevel[l], nt = nt_of(kLayers[l].cout), cin = kLayers[l].cin;
@@ -623,7 +663,12 @@ bool backward(LBMWarmNet *n, const float *target_dev, int nb) {
         w.chunks_per_split = sp.chunks;
         if (!ok(n, conv_wgrad(w, nt, sp.splits, n->grad + n->woff[l], 0, s, kLayers[l].cout)))
             return false;
-        k_bias_grad<<<kLayers[l].cout, 256, 0, s>>>(n->g, nt, m, n->grad + n->boff[l]);
+        {
+            const unsigned bb = nblk(m, BG_ROWS);
+            k_bias_grad_part<<<bb, 256, 0, s>>>(n->g, nt, m, n->bias_part);
+            k_bias_grad_sum<<<1, 256, 0, s>>>(n->bias_part, (int)bb, nt, kLayers[l].cout,
+                                              n->grad + n->boff[l]);
+        }
         if (!ok(n, cudaGetLastError())) return false;
         // input gradient
         if (l > 0) {
@@ -780,6 +825,14 @@ LBMWarmNet *LBM_WarmNetCreate(int nx, int ny, int nz, int maxBatch, unsigned see
     n->pred32 = n->alloc<float>(m1 * 4);
     n->loss = n->alloc<double>(1);
     n->sq = n->alloc<double>(1);
+    {
+        long long bp = 0;  // largest (blocks x nt) of the bias-gradient partials
+        for (int l = 0; l < NLAYERS; l++) {
+            const long long b = (n->m(kLevel[l], B) + BG_ROWS - 1) / BG_ROWS;
+            bp = b * nt_of(kLayers[l].cout) > bp ? b * nt_of(kLayers[l].cout) : bp;
+        }
+        n->bias_part = n->alloc<float>(bp);
+    }
     if (n->error) {
         LBM_WarmNetFree(n);
         return nullptr;

@@ -474,20 +474,50 @@ __host__ __device__ constexpr int pair_minb() {
     return SMAG ? 6 : 7;
 #endif
 }
-// Batched launches read each grid's arguments from shared memory and hold
-// more registers; they are capped at 96 (5 blocks per SM) unless
-// LBM_PAIR_MINB_BATCH says otherwise (measurements).
+// Batched launches of one operator take that operator's cap; a launch that
+// switches between operators at run time holds the largest of them and is
+// capped at 96 registers (5 blocks per SM).  LBM_PAIR_MINB_BATCH overrides
+// (measurements).
 __host__ __device__ constexpr int pair_minb_set(int set) {
 #ifdef LBM_PAIR_MINB_BATCH
     return (void)set, LBM_PAIR_MINB_BATCH;
 #else
-    return (void)set, 5;
+    return set == BATCH_SET_BGK || set == BATCH_SET_REG || set == BATCH_SET_MRT ? 7
+           : set < BATCH_SET_BGK_REG                                          ? 6
+                                                                               : 5;
 #endif
 }
 
 // Where the scalar fallback parks the second cell of a pair (one array per
 // kernel, whichever operators the kernel instantiates).
 __shared__ float pair_park[19 * PAIR_THREADS];
+
+// Where a pair's populations come from and go to.  TabParam reads the
+// per-direction pointers precomputed in a kernel parameter (constant-bank
+// operands, no registers); TabCalc computes them from the two buffers'
+// bases and the grid's extents, holding a few scalars instead of 57
+// pointers -- for kernels whose grid is chosen at run time.
+struct TabParam {
+    const PairTable &t;
+    __device__ __forceinline__ const void *pull(int i) const { return t.pull[i]; }
+    __device__ __forceinline__ const void *own(int i) const { return t.own[i]; }
+    __device__ __forceinline__ void *dst(int i) const { return t.dst[i]; }
+    __device__ __forceinline__ float2 nz() const { return t.nz; }
+};
+
+template <class T>
+struct TabCalc {
+    const T *src;
+    T *dstb;
+    int n, nx, plane;
+    float2 z;
+    __device__ __forceinline__ const void *own(int i) const { return src + (long long)i * n; }
+    __device__ __forceinline__ const void *pull(int i) const {
+        return src + ((long long)i * n - cx(i) - cy(i) * nx - cz(i) * plane);
+    }
+    __device__ __forceinline__ void *dst(int i) const { return dstb + (long long)i * n; }
+    __device__ __forceinline__ float2 nz() const { return z; }
+};
 
 template <class S>
 __device__ __forceinline__ void pair_load(const void *base, unsigned cell, int i, float &a,
@@ -506,18 +536,18 @@ __device__ __forceinline__ void pair_load(const void *base, unsigned cell, int i
 // the reference's x-edge rule by a per-lane pointer select: a cell whose
 // source x lies outside the grid keeps its own value (lbm_stream.comp:
 // 116-127).  Calls copy(i, lane-x source, lane-y source, aligned pair).
-template <class S, class Copy>
-__device__ __forceinline__ void pair_pull_interior(const StepArgs &a, const PairTable &t,
-                                                   int x0, unsigned cell0, Copy copy) {
+template <class S, class Tab, class Copy>
+__device__ __forceinline__ void pair_pull_interior(const StepArgs &a, const Tab &t, int x0,
+                                                   unsigned cell0, Copy copy) {
     using T = typename S::T;
     const bool edgeA = x0 == 0, edgeB = x0 + 2 == a.nx;
 #pragma unroll
     for (int i = 0; i < 19; i++) {
-        const T *pull = static_cast<const T *>(t.pull[i]) + cell0;
+        const T *pull = static_cast<const T *>(t.pull(i)) + cell0;
         if (cx(i) == 0) {
             copy(i, pull, pull + 1, true);
         } else {
-            const T *own = static_cast<const T *>(t.own[i]) + cell0;
+            const T *own = static_cast<const T *>(t.own(i)) + cell0;
             const bool keepA = cx(i) == 1 && edgeA, keepB = cx(i) == -1 && edgeB;
             copy(i, keepA ? own : pull, keepB ? own + 1 : pull + 1, false);
         }
@@ -527,8 +557,8 @@ __device__ __forceinline__ void pair_pull_interior(const StepArgs &a, const Pair
 // The populations of one pair before Bouzidi: FUSED, the pull (interior
 // row or, on a y / z face row, the wrap / clamp rules of gather_pull);
 // otherwise the buffer's own values (the first step after initialisation).
-template <class S, bool FUSED>
-__device__ __forceinline__ void pair_gather(const StepArgs &a, const PairTable &t, int x0, int y,
+template <class S, bool FUSED, class Tab>
+__device__ __forceinline__ void pair_gather(const StepArgs &a, const Tab &t, int x0, int y,
                                             int z, unsigned cell0, float (&fa)[19],
                                             float (&fb)[19]) {
     using T = typename S::T;
@@ -551,14 +581,14 @@ __device__ __forceinline__ void pair_gather(const StepArgs &a, const PairTable &
         }
     } else {
 #pragma unroll
-        for (int i = 0; i < 19; i++) pair_load<S>(t.own[i], cell0, i, fa[i], fb[i], true);
+        for (int i = 0; i < 19; i++) pair_load<S>(t.own(i), cell0, i, fa[i], fb[i], true);
     }
 }
 
 // Bouzidi on the pair's link-owning cells (FUSED), the collision and the
 // store of one pair; returns the pair's guard resets.
-template <class S, int OP, bool SMAG, bool FUSED>
-__device__ __forceinline__ int pair_finish(const StepArgs &a, const PairTable &t, int x0, int y,
+template <class S, int OP, bool SMAG, bool FUSED, class Tab>
+__device__ __forceinline__ int pair_finish(const StepArgs &a, const Tab &t, int x0, int y,
                                            int z, unsigned cell0, uint8_t flagA, uint8_t flagB,
                                            float (&fa)[19], float (&fb)[19]) {
     using T = typename S::T;
@@ -591,17 +621,17 @@ __device__ __forceinline__ int pair_finish(const StepArgs &a, const PairTable &t
             resets += kind == 2;
 #pragma unroll
             for (int i = 0; i < 19; i++)
-                S::store(static_cast<T *>(t.dst[i]) + cell0 + c, fn[i], i);
+                S::store(static_cast<T *>(t.dst(i)) + cell0 + c, fn[i], i);
         }
     } else {
         P fn[19];
         bool resetA, resetB;
         pair_collide_fluid<OP, SMAG>(fa, fb, x0 == 0, x0 + 1 == a.nx - 1, a.inX, a.inY, a.inZ,
-                                     a.tau, a.omega, a.smag18, t.nz, fn, resetA, resetB);
+                                     a.tau, a.omega, a.smag18, t.nz(), fn, resetA, resetB);
         resets = (int)resetA + (int)resetB;
 #pragma unroll
         for (int i = 0; i < 19; i++)
-            S::store2(static_cast<T *>(t.dst[i]) + cell0, fn[i].x, fn[i].y, i);
+            S::store2(static_cast<T *>(t.dst(i)) + cell0, fn[i].x, fn[i].y, i);
     }
     return resets;
 }
@@ -621,9 +651,8 @@ __device__ __forceinline__ void pair_count_resets(const StepArgs &a, int resets)
 // One thread: the cells (x0, y, z) and (x0 + 1, y, z), x0 even.  FUSED:
 // pull-stream (+ Bouzidi) then collide; otherwise collide the buffer's own
 // values (the first step after initialisation).
-template <class S, int OP, bool SMAG, bool FUSED>
-__device__ __forceinline__ void step_pair(const StepArgs &a, const PairTable &t, int x0, int y,
-                                          int z) {
+template <class S, int OP, bool SMAG, bool FUSED, class Tab>
+__device__ __forceinline__ void step_pair(const StepArgs &a, const Tab &t, int x0, int y, int z) {
     if (x0 >= a.nx || y >= a.ny) return;
     const unsigned cell0 = (unsigned)x0 + (unsigned)a.nx * ((unsigned)y + (unsigned)a.ny * z);
     const uchar2 fl = *reinterpret_cast<const uchar2 *>(a.flags + cell0);
@@ -638,17 +667,20 @@ __device__ __forceinline__ void step_pair(const StepArgs &a, const PairTable &t,
 template <class S, int OP, bool SMAG, bool FUSED>
 __global__ void __launch_bounds__(PAIR_THREADS, pair_minb<OP, SMAG>())
     k_step_pair(const StepArgs a, const __grid_constant__ PairTable t) {
-    step_pair<S, OP, SMAG, FUSED>(a, t, 2 * (blockIdx.x * blockDim.x + threadIdx.x),
+    step_pair<S, OP, SMAG, FUSED>(a, TabParam{t}, 2 * (blockIdx.x * blockDim.x + threadIdx.x),
                                   blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z);
 }
 
 // Batched paired step: one launch advances up to BATCH_LAUNCH_MAX grids by
 // one fused step.  Work unit: one tile of one z-plane of one grid, one
 // PAIR_THREADS block per unit; the block finds its grid by binary search over
-// the unit offsets and copies that grid's entry (step arguments, pointer
-// table, operator, tile shape) from the device table into shared memory, so
-// nothing is indexed at run time in the parameter space.  The per-cell code
-// is k_step_pair's, so every grid's result is bit-identical to a solo step.
+// the unit offsets and copies that grid's entry (step arguments, operator,
+// tile shape) from the device table into shared memory, so nothing is
+// indexed at run time in the parameter space; the per-direction pointers
+// are computed from the buffers' bases (TabCalc) rather than read from the
+// entry's table, which would hold 57 pointers in registers.  The per-cell
+// code is k_step_pair's, so every grid's result is bit-identical to a solo
+// step.
 template <class S, int SET>
 __global__ void __launch_bounds__(PAIR_THREADS, pair_minb_set(SET))
     k_step_batch_pair(const __grid_constant__ BatchPairParams p) {
@@ -675,14 +707,17 @@ __global__ void __launch_bounds__(PAIR_THREADS, pair_minb_set(SET))
     const int bxt = 1 << g.lbx;
     const int x0 = 2 * ((int)tx * bxt + (int)(threadIdx.x & (bxt - 1)));
     const int y = ty * (PAIR_THREADS >> g.lbx) + (int)(threadIdx.x >> g.lbx);
+    using T = typename S::T;
+    const TabCalc<T> t{static_cast<const T *>(g.a.src), static_cast<T *>(g.a.dst), (int)g.a.n,
+                       g.a.nx, g.a.nx * g.a.ny, g.t.nz};
     constexpr unsigned M = batch_set_mask(SET);
     switch (g.combo) {
-        case 0: if constexpr ((M & 1u) != 0) step_pair<S, OP_BGK, false, true>(g.a, g.t, x0, y, z); break;
-        case 1: if constexpr ((M & 2u) != 0) step_pair<S, OP_BGK, true, true>(g.a, g.t, x0, y, z); break;
-        case 2: if constexpr ((M & 4u) != 0) step_pair<S, OP_REG, false, true>(g.a, g.t, x0, y, z); break;
-        case 3: if constexpr ((M & 8u) != 0) step_pair<S, OP_REG, true, true>(g.a, g.t, x0, y, z); break;
-        case 4: if constexpr ((M & 16u) != 0) step_pair<S, OP_MRT, false, true>(g.a, g.t, x0, y, z); break;
-        default: if constexpr ((M & 32u) != 0) step_pair<S, OP_MRT, true, true>(g.a, g.t, x0, y, z); break;
+        case 0: if constexpr ((M & 1u) != 0) step_pair<S, OP_BGK, false, true>(g.a, t, x0, y, z); break;
+        case 1: if constexpr ((M & 2u) != 0) step_pair<S, OP_BGK, true, true>(g.a, t, x0, y, z); break;
+        case 2: if constexpr ((M & 4u) != 0) step_pair<S, OP_REG, false, true>(g.a, t, x0, y, z); break;
+        case 3: if constexpr ((M & 8u) != 0) step_pair<S, OP_REG, true, true>(g.a, t, x0, y, z); break;
+        case 4: if constexpr ((M & 16u) != 0) step_pair<S, OP_MRT, false, true>(g.a, t, x0, y, z); break;
+        default: if constexpr ((M & 32u) != 0) step_pair<S, OP_MRT, true, true>(g.a, t, x0, y, z); break;
     }
 }
 

@@ -2,7 +2,7 @@
 
 The network is trained, by this library's own forward and backward kernels,
 on snapshots that the plain solver produces for 64 random shapes (seed 2) at
-64x32x32; then, on 8 held-out shapes at 128x64x64, the number of steps until
+64x32x32 (300 epochs); then, on 8 held-out shapes at 128x64x64, the number of steps until
 the trailing-mean drag coefficient enters and stays within 0.5 % of its
 converged value (the mean of a long cold run) is compared for (a) the plain
 method, uniform flow at start, and (b) the same solver initialised from the
@@ -33,8 +33,10 @@ def test_trained_warm_start_reaches_the_cd_band_sooner(solver):
     from lattice_fluid_dynamics_b200 import warmstart as W
     net = capi.WarmNet(*NET, max_batch=8, seed=2)
     info = {}
+    # 56 training samples, batch 8: 7 Adam steps per epoch; 300 epochs get
+    # past the 200-step learning-rate warm-up into the cosine decay
     hist = W.train_from_snapshots(net, count=64, val=8, seed=2, snapshot_dims=HALF,
-                                  snapshot_steps=4000, epochs=30, batch=8, lr=3e-4, res=info)
+                                  snapshot_steps=4000, epochs=300, batch=8, lr=1e-3, res=info)
     assert hist[-1]["train_loss"] < 0.5 * hist[0]["train_loss"], hist
     shapes = [W.random_union(2, 100000 + i) for i in range(8)]
     rows = _evaluate(net, shapes)
