@@ -381,12 +381,14 @@ int LBM_NNConvWeightGrad(const void *x, int xStride, int xOff, int cin, const vo
  * waiting for its tensor-core work since the last call, else LBM_OK. */
 int LBM_NNTakeError(void);
 
-/* Which forward / input-gradient kernel LBM_NNConvForward and the network
- * use: 0 (default) the halo-tiled kernel wherever the shape allows it (input
- * channels a multiple of 16, NX a multiple of 8, NY a multiple of 16,
- * coutPad 16 / 32 / 48 / 64 / 96) and the im2col-gather kernel elsewhere;
- * 1 the gather kernel for every shape.  Process-wide; not thread-safe
- * against concurrent launches.  LBM_OK or LBM_ERR_INVALID_ARGUMENT. */
+/* Which convolution kernels LBM_NNConvForward, LBM_NNConvWeightGrad and
+ * the network use: 0 (default) the halo-tiled forward kernel wherever the
+ * shape allows it (input channels a multiple of 16, NX a multiple of 8, NY
+ * a multiple of 16, coutPad 16 / 32 / 48 / 64 / 96) and the cp.async-
+ * pipelined im2col kernels elsewhere (and for every weight gradient); 1 the
+ * original synchronous im2col kernels for every shape; 2 the pipelined
+ * im2col kernels for every shape.  Process-wide; not thread-safe against
+ * concurrent launches.  LBM_OK or LBM_ERR_INVALID_ARGUMENT. */
 int LBM_NNSetConvPath(int path);
 
 /* The warm-start network: a 4-level 3D conv encoder-decoder (8->16->32->64

@@ -266,31 +266,11 @@ bool step_fused(LBMBatch &b, const std::vector<BatchLaunchParams> &p, const std:
     return true;
 }
 
-// The paired kernel's pointer table for step arguments a (element size elem).
-PairTable pair_table_of(const StepArgs &a, size_t elem) {
-    PairTable t;
-    const char *src = static_cast<const char *>(a.src);
-    char *dst = static_cast<char *>(a.dst);
-    const long long plane = (long long)a.nx * a.ny;
-    static const int ex[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
-    static const int ey[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
-    static const int ez[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
-    for (int i = 0; i < 19; i++) {
-        const long long own = (long long)i * a.n;
-        const long long shift = ex[i] + ey[i] * (long long)a.nx + ez[i] * plane;
-        t.own[i] = src + own * (long long)elem;
-        t.pull[i] = src + (own - shift) * (long long)elem;
-        t.dst[i] = dst + own * (long long)elem;
-    }
-    t.nz = make_float2(-0.0f, -0.0f);
-    return t;
-}
-
 BatchGridDev pair_entry(LBMBatch &b, int i, const StepArgs &a) {
     BatchGridDev e;
     memset(&e, 0, sizeof(e));  // padding too: entries are compared bytewise
     e.a = a;
-    e.t = pair_table_of(a, impl(b.grids[i])->elem);
+    e.nz = make_float2(-0.0f, -0.0f);
     e.combo = combo_of(b.grids[i]);
     e.lbx = b.lbx[i];
     e.tiles_x = (impl(b.grids[i])->nx + tile_x_cells(b, e.lbx) - 1) / tile_x_cells(b, e.lbx);

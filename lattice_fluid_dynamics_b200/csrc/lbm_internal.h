@@ -146,10 +146,11 @@ struct PairTable {
 
 // One grid of a batched paired step launch (k_step_batch_pair), kept in
 // device memory (one table per buffer parity) and copied into shared memory
-// by each block that works on the grid.
+// by each block that works on the grid.  The kernel computes the
+// per-direction pointers from a.src / a.dst and the extents.
 struct alignas(16) BatchGridDev {
     StepArgs a;
-    PairTable t;
+    float2 nz;    // (-0, -0): addend of the paired products
     int combo;    // op * 2 + smagorinsky
     int lbx;      // 1 << lbx threads along x (two cells each), 128 >> lbx rows
     int tiles_x;

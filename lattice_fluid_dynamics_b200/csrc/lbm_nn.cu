@@ -12,6 +12,7 @@
 #include "lbm_nn.h"
 #include "lbm_nn_gemm.cuh"
 #include "lbm_nn_halo.cuh"
+#include "lbm_nn_wgrad.cuh"
 
 namespace lbm {
 namespace nn {
@@ -93,6 +94,11 @@ float *split_workspace(cudaStream_t s, size_t bytes) {
     return static_cast<float *>(b.first);
 }
 
+// Launch of the forward gather GEMM: the cp.async-pipelined kernel, or the
+// original synchronous one (LBM_NNSetConvPath(1)).
+template <int NT>
+cudaError_t launch_fwd_gather(const ConvFwdArgs &a, dim3 grid, cudaStream_t s);
+
 template <int NT>
 cudaError_t fwd_nt(ConvFwdArgs a, int slot, cudaStream_t s) {
     cudaError_t e = set_attr<NT>(slot);
@@ -114,19 +120,22 @@ cudaError_t fwd_nt(ConvFwdArgs a, int slot, cudaStream_t s) {
         if (ws) {
             a.partial = ws;
             a.chunks_per_split = cps;
-            k_conv_fwd<NT><<<dim3(blocks, (unsigned)splits), 128, gemm_smem_bytes<NT>(), s>>>(a);
+            e = launch_fwd_gather<NT>(a, dim3(blocks, (unsigned)splits), s);
+            if (e != cudaSuccess) return e;
             const long long outs = a.m * (a.cout_store / 8);
             k_conv_fwd_finish<<<(unsigned)((outs + 255) / 256), 256, 0, s>>>(a, NT, splits);
             return cudaGetLastError();
         }
     }
     a.partial = nullptr;
-    k_conv_fwd<NT><<<blocks, 128, gemm_smem_bytes<NT>(), s>>>(a);
-    return cudaGetLastError();
+    return launch_fwd_gather<NT>(a, dim3(blocks), s);
 }
 
-// 0: the halo-tiled forward kernel where a convolution's shape allows it;
-// 1: the gather kernel for every shape (LBM_NNSetConvPath, for comparisons)
+// 0: the halo-tiled forward kernel where a convolution's shape allows it,
+//    the cp.async-pipelined gather kernels elsewhere;
+// 1: the original synchronous gather kernels for every shape;
+// 2: the pipelined gather kernels for every shape
+// (LBM_NNSetConvPath, for comparisons)
 int g_conv_path = 0;
 
 bool halo_shape_ok(const ConvFwdArgs &a, int nt) {
@@ -144,6 +153,10 @@ cudaError_t fwd_halo_nt(ConvFwdArgs a, cudaStream_t s) {
     std::call_once(once, [] {
         attr = cudaFuncSetAttribute(k_conv_fwd_halo<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     halo_smem_bytes<NT>());
+        if (attr == cudaSuccess)
+            attr = cudaFuncSetAttribute(k_conv_fwd_halo<NT>,
+                                        cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        cudaSharedmemCarveoutMaxShared);
         int dev = 0;
         if (attr == cudaSuccess) attr = cudaGetDevice(&dev);
         if (attr == cudaSuccess)
@@ -161,40 +174,43 @@ cudaError_t fwd_halo_nt(ConvFwdArgs a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-bool wgrad_halo_ok(const ConvWgradArgs &a, int nt) {
-    return g_conv_path == 0 && a.cin % 16 == 0 && a.x_stride % 8 == 0 && a.x_off % 8 == 0 &&
-           a.g_stride % 8 == 0 && a.g_stride >= nt && a.d.nx % 8 == 0 && a.d.ny % 16 == 0 &&
-           (nt == 16 || nt == 32 || nt == 64 || nt == 128) &&
-           (long long)a.d.nb * a.d.nz * (a.d.ny / 16) * (a.d.nx / 8) < (1ll << 31);
-}
-
-// Runs k_conv_wgrad_halo with at most `splits` tile ranges (the partial
-// workspace holds that many); returns the number used in *used.
 template <int NT>
-cudaError_t wgrad_halo_nt(ConvWgradArgs a, unsigned splits, unsigned *used, cudaStream_t s) {
+cudaError_t launch_fwd_gather(const ConvFwdArgs &a, dim3 grid, cudaStream_t s) {
+    if (g_conv_path == 1 || a.m >= (1ll << 31)) {
+        k_conv_fwd<NT><<<grid, 128, gemm_smem_bytes<NT>(), s>>>(a);
+        return cudaGetLastError();
+    }
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
-    static int sms = 0;
     std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(k_conv_wgrad_halo<NT>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, WG_SMEM_BYTES);
-        int dev = 0;
-        if (attr == cudaSuccess) attr = cudaGetDevice(&dev);
+        attr = cudaFuncSetAttribute(k_conv_fwd_async<NT>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    fwdas_smem_bytes<NT>());
         if (attr == cudaSuccess)
-            attr = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            attr = cudaFuncSetAttribute(k_conv_fwd_async<NT>,
+                                        cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        cudaSharedmemCarveoutMaxShared);
     });
     if (attr != cudaSuccess) return attr;
-    const long long tiles = (long long)a.d.nb * a.d.nz * (a.d.ny / 16) * (a.d.nx / 8);
-    const int slices = a.cin / 16;
-    long long sp = (sms + slices - 1) / slices;  // one CTA per SM (512 TMEM columns each)
-    if (sp > (long long)splits) sp = splits;
-    if (sp > tiles) sp = tiles;
-    if (sp < 1) sp = 1;
-    const long long per = (tiles + sp - 1) / sp;
-    sp = (tiles + per - 1) / per;
-    k_conv_wgrad_halo<NT><<<dim3(slices, (unsigned)sp), 128, WG_SMEM_BYTES, s>>>(a, (int)tiles,
-                                                                                 (int)per);
-    *used = (unsigned)sp;
+    k_conv_fwd_async<NT><<<grid, 128, fwdas_smem_bytes<NT>(), s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int NT>
+cudaError_t wgrad_mn_nt(const ConvWgradArgs &a, unsigned splits, cudaStream_t s) {
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_conv_wgrad_mn<NT>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    wgmn_smem_bytes<NT>());
+        if (attr == cudaSuccess)
+            attr = cudaFuncSetAttribute(k_conv_wgrad_mn<NT>,
+                                        cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        cudaSharedmemCarveoutMaxShared);
+    });
+    if (attr != cudaSuccess) return attr;
+    k_conv_wgrad_mn<NT><<<dim3(a.k_pad / 128, splits), 128, wgmn_smem_bytes<NT>(), s>>>(a);
     return cudaGetLastError();
 }
 
@@ -208,17 +224,27 @@ cudaError_t wgrad_nt(ConvWgradArgs a, int slot, unsigned splits, cudaStream_t s)
 }
 
 
-// dW[n][k] = sum over splits of partial[split][k][n], n < cout, k < k_real
-// (thread i = k * cout + n: a warp reads contiguous partials)
+// dW[n][k] = sum over splits of partial[split][k][n], n < cout, k < k_real.
+// Eight threads per output: thread r sums splits r, r + 8, ... and the
+// eight are combined by a fixed shuffle tree (deterministic); consecutive
+// outputs are consecutive n, so a warp reads contiguous partials.
 __global__ void k_wgrad_reduce(const float *__restrict__ partial, int splits, int k_pad, int nt,
                                int cout, int k_real, float *__restrict__ dw, int accumulate) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= cout * k_real) return;
-    const int k = i / cout, n = i - k * cout;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = (int)(t & 7);
+    const long long i = t >> 3;  // output index k * cout + n
+    const bool live = i < (long long)cout * k_real;
+    const int k = live ? (int)(i / cout) : 0, n = live ? (int)(i - (long long)k * cout) : 0;
     float s = 0.f;
-    for (int p = 0; p < splits; p++) s += partial[((long long)p * k_pad + k) * nt + n];
-    float *o = dw + (long long)n * k_real + k;
-    *o = accumulate ? *o + s : s;
+    if (live)
+        for (int p = r; p < splits; p += 8) s += partial[((long long)p * k_pad + k) * nt + n];
+    s += __shfl_down_sync(0xffffffffu, s, 4, 8);
+    s += __shfl_down_sync(0xffffffffu, s, 2, 8);
+    s += __shfl_down_sync(0xffffffffu, s, 1, 8);
+    if (live && r == 0) {
+        float *o = dw + (long long)n * k_real + k;
+        *o = accumulate ? *o + s : s;
+    }
 }
 
 // Wt[ci][(26 - tap) * cout + co] = W[co][tap * cin + ci]  (flip and transpose)
@@ -264,20 +290,24 @@ cudaError_t conv_forward(const ConvFwdArgs &a0, int nt, cudaStream_t s) {
 }
 
 cudaError_t conv_wgrad(const ConvWgradArgs &a0, int nt, unsigned splits, float *dw,
-                       int accumulate, cudaStream_t s, int cout_write) {
+                       int accumulate, cudaStream_t s, int cout_write, float *dbias,
+                       bool *bias_done) {
     ConvWgradArgs a = a0;
     a.err = err_ptr();
     if (!a.err) return cudaErrorInvalidDevicePointer;
+    if (bias_done) *bias_done = false;
+    const bool mn = g_conv_path != 1 && a.m < (1ll << 31);
+    // the bias gradient rides on the first padding row group, if it exists
+    a.ones_row = (mn && dbias && a.k_pad - a.k_real >= 8 && a.k_real % 8 == 0) ? a.k_real : -1;
     cudaError_t e;
-    if (wgrad_halo_ok(a, nt)) {
-        unsigned used = splits;
+    if (mn) {
         switch (nt) {
-            case 16: e = wgrad_halo_nt<16>(a, splits, &used, s); break;
-            case 32: e = wgrad_halo_nt<32>(a, splits, &used, s); break;
-            case 64: e = wgrad_halo_nt<64>(a, splits, &used, s); break;
-            default: e = wgrad_halo_nt<128>(a, splits, &used, s); break;
+            case 16: e = wgrad_mn_nt<16>(a, splits, s); break;
+            case 32: e = wgrad_mn_nt<32>(a, splits, s); break;
+            case 64: e = wgrad_mn_nt<64>(a, splits, s); break;
+            case 128: e = wgrad_mn_nt<128>(a, splits, s); break;
+            default: return cudaErrorInvalidValue;
         }
-        splits = used;
     } else {
         switch (nt) {
             case 16: e = wgrad_nt<16>(a, 0, splits, s); break;
@@ -289,9 +319,16 @@ cudaError_t conv_wgrad(const ConvWgradArgs &a0, int nt, unsigned splits, float *
     }
     if (e != cudaSuccess) return e;
     const int rows = cout_write > 0 ? cout_write : a.cout;
-    const int total = rows * a.k_real;
-    k_wgrad_reduce<<<(total + 255) / 256, 256, 0, s>>>(a.partial, (int)splits, a.k_pad, nt,
-                                                       rows, a.k_real, dw, accumulate);
+    const long long total = 8ll * rows * a.k_real;
+    k_wgrad_reduce<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(
+        a.partial, (int)splits, a.k_pad, nt, rows, a.k_real, dw, accumulate);
+    if (a.ones_row >= 0) {
+        // db[n] = sum over splits of partial[split][ones_row][n]: the same
+        // reduction as one more row of dW, written to a [rows][1] matrix
+        k_wgrad_reduce<<<(unsigned)((8 * rows + 255) / 256), 256, 0, s>>>(
+            a.partial + (long long)a.ones_row * nt, (int)splits, a.k_pad, nt, rows, 1, dbias, 0);
+        if (bias_done) *bias_done = true;
+    }
     return cudaGetLastError();
 }
 
@@ -405,7 +442,7 @@ int LBM_NNConvWeightGrad(const void *x, int xStride, int xOff, int cin, const vo
 int LBM_NNTakeError(void) { return take_error() ? LBM_ERR_TIMEOUT : LBM_OK; }
 
 int LBM_NNSetConvPath(int path) {
-    if (path != 0 && path != 1) return LBM_ERR_INVALID_ARGUMENT;
+    if (path < 0 || path > 2) return LBM_ERR_INVALID_ARGUMENT;
     g_conv_path = path;
     return LBM_OK;
 }

@@ -14,9 +14,13 @@ struct ConvWgradArgs;
 // K (27 taps x cin) rounded up to a multiple of 128
 int k_pad_of(int cin);
 cudaError_t conv_forward(const ConvFwdArgs &a, int nt, cudaStream_t s);
-// dw rows written: cout_write (> 0) or a.cout
+// dw rows written: cout_write (> 0) or a.cout.  With dbias set, the bias
+// gradient (the sum of g over voxels) is written there too when the kernel
+// can fold it into the weight gradient (*bias_done = true); otherwise the
+// caller computes it.
 cudaError_t conv_wgrad(const ConvWgradArgs &a, int nt, unsigned splits, float *dw, int accumulate,
-                       cudaStream_t s, int cout_write = 0);
+                       cudaStream_t s, int cout_write = 0, float *dbias = nullptr,
+                       bool *bias_done = nullptr);
 cudaError_t weight_transpose(const __nv_bfloat16 *w, int cout, int cin, __nv_bfloat16 *wt,
                              int wt_rows, cudaStream_t s);
 // reads and clears the device error word of the GEMM kernels (synchronous)

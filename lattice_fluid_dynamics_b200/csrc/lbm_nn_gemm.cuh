@@ -95,6 +95,10 @@ struct ConvWgradArgs {
     long long m;
     int chunks_per_split;    // reduction slices of KC voxels per CTA
     int *err;
+    // >= 0: reduction rows [ones_row, ones_row + 8) read 1.0 instead of x, so
+    // that partial row ones_row sums the gradient itself (the bias gradient);
+    // a padding row (k_real <= ones_row < k_pad)
+    int ones_row;
 };
 
 // ---------------------------------------------------------------------------

@@ -50,7 +50,11 @@ constexpr int HALO_BYTES = 2 * HPLANE;    // one 16-channel slice
 
 template <int NT>
 __host__ __device__ constexpr int halo_stages() {
+#ifdef LBM_HALO_STAGES16
+    return NT <= 16 ? LBM_HALO_STAGES16 : 2;
+#else
     return NT <= 16 ? 3 : 2;
+#endif
 }
 template <int NT>
 __host__ __device__ constexpr int halo_stage_bytes() {
@@ -123,29 +127,52 @@ __global__ void __launch_bounds__(128) k_conv_fwd_halo(const ConvFwdArgs a, int 
     const int my_tiles = (int)blockIdx.x < tiles ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     const int nq = my_tiles * ck;
 
-    // all threads: copies of work item q (tile q / ck, slice q % ck) into stage q % S
+    // This thread's halo elements e = tid + 128 i: shared-memory offset,
+    // position in the halo and voxel offset from the halo's (1, 1, 1) corner
+    // -- the same for every tile.
+    constexpr int HE = (2 * HVOX + 127) / 128;
+    uint32_t h_soff[HE];
+    int h_pos[HE];   // hx | hy << 8 | hz << 16 | kc << 24, or -1 past the end
+    int h_rel[HE];   // voxel offset
+#pragma unroll
+    for (int i = 0; i < HE; i++) {
+        const int e = tid + 128 * i;
+        const int kc = e >= HVOX, v = e - kc * HVOX;
+        const int hx = v % HX, hy = (v / HX) % HY, hz = v / (HX * HY);
+        h_soff[i] = (uint32_t)(kc * HPLANE + v * 16);
+        h_pos[i] = e < 2 * HVOX ? (hx | hy << 8 | hz << 16 | kc << 24) : -1;
+        h_rel[i] = ((hz - 1) * a.d.ny + (hy - 1)) * a.d.nx + (hx - 1);
+    }
+
+    // all threads: copies of work item q (tile q / ck, slice q % ck) into
+    // stage q % S; with a single slice the weights are copied once (item 0,
+    // stage 0) and stay there
     auto issue = [&](int q) {
         const int i = q / ck, j = q - i * ck;
         const HaloTile t = halo_tile(a.d, (int)blockIdx.x + i * (int)gridDim.x);
-        uint8_t *st = smem + (q % S) * SB;
-        const uint32_t st_addr = tc::smem_addr(st);
-        for (int e = tid; e < 2 * HVOX; e += 128) {
-            const int kc = e >= HVOX, v = e - kc * HVOX;
-            const int hx = v % HX, hy = (v / HX) % HY, hz = v / (HX * HY);
+        const uint32_t st_addr = tc::smem_addr(smem + (q % S) * SB);
+        const long long base =
+            (((long long)t.b * a.d.nz + t.z) * a.d.ny + t.ty * 16) * a.d.nx + t.tx * 8;
+        const __nv_bfloat16 *xs = a.x + a.x_off + j * 16;
+#pragma unroll
+        for (int k = 0; k < HE; k++) {
+            if (h_pos[k] < 0) break;
+            const int hx = h_pos[k] & 255, hy = (h_pos[k] >> 8) & 255,
+                      hz = (h_pos[k] >> 16) & 255, kc = h_pos[k] >> 24;
             const int gx = t.tx * 8 + hx - 1, gy = t.ty * 16 + hy - 1, gz = t.z + hz - 1;
-            const bool in = gx >= 0 && gx < a.d.nx && gy >= 0 && gy < a.d.ny && gz >= 0 &&
-                            gz < a.d.nz;
-            const long long vox =
-                in ? (((long long)t.b * a.d.nz + gz) * a.d.ny + gy) * a.d.nx + gx : 0;
-            cp_async16(st_addr + kc * HPLANE + v * 16,
-                       a.x + vox * a.x_stride + a.x_off + j * 16 + kc * 8, in ? 16u : 0u);
+            const bool in = (unsigned)gx < (unsigned)a.d.nx && (unsigned)gy < (unsigned)a.d.ny &&
+                            (unsigned)gz < (unsigned)a.d.nz;
+            const long long vox = in ? base + h_rel[k] : 0;
+            cp_async16(st_addr + h_soff[k], xs + vox * a.x_stride + kc * 8, in ? 16u : 0u);
         }
-        const uint32_t w_addr = st_addr + HALO_BYTES;
-        for (int e = tid; e < 54 * NT; e += 128) {
-            const int n = e % NT, tk = e / NT;  // tk = tap * 2 + plane
-            cp_async16(w_addr + (tk * NT + n) * 16,
-                       a.w + (long long)n * a.k_pad + (tk >> 1) * a.cin + j * 16 + (tk & 1) * 8,
-                       16u);
+        if (ck > 1 || q == 0) {
+            const uint32_t w_addr = st_addr + HALO_BYTES;
+            for (int e = tid; e < 54 * NT; e += 128) {
+                const int n = e % NT, tk = e / NT;  // tk = tap * 2 + plane
+                cp_async16(w_addr + (tk * NT + n) * 16,
+                           a.w + (long long)n * a.k_pad + (tk >> 1) * a.cin + j * 16 + (tk & 1) * 8,
+                           16u);
+            }
         }
     };
 
@@ -164,14 +191,18 @@ __global__ void __launch_bounds__(128) k_conv_fwd_halo(const ConvFwdArgs a, int 
         __syncthreads();
         tc::fence_after_sync();
         if (tid == 0) {
-            const uint32_t hb = tc::smem_addr(smem + s * SB), wb = hb + HALO_BYTES;
-#pragma unroll 1
+            // descriptors of tap 0; a tap moves only the start address, which
+            // is the descriptor's low field in 16-byte units (no carry: shared
+            // addresses stay below 256 KB)
+            const uint32_t hb = tc::smem_addr(smem + s * SB);
+            const uint32_t wb = tc::smem_addr(smem + (ck > 1 ? s : 0) * SB) + HALO_BYTES;
+            const uint64_t a0 = tc::kmajor_desc(hb, HPLANE, HX * 16);
+            const uint64_t b0 = tc::kmajor_desc(wb, NT * 16, 128);
+#pragma unroll
             for (int tap = 0; tap < 27; tap++) {
                 const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
-                const uint64_t ad =
-                    tc::kmajor_desc(hb + ((dz * HY + dy) * HX + dx) * 16, HPLANE, HX * 16);
-                const uint64_t bd = tc::kmajor_desc(wb + tap * 2 * NT * 16, NT * 16, 128);
-                tc::mma_bf16(tmem, ad, bd, idesc, (j | tap) != 0);
+                tc::mma_bf16(tmem, a0 + (uint64_t)((dz * HY + dy) * HX + dx),
+                             b0 + (uint64_t)(tap * 2 * NT), idesc, (j | tap) != 0);
             }
             tc::mma_commit(bar_stage(s));
             if (j == ck - 1) tc::mma_commit(bar_acc);
@@ -233,178 +264,6 @@ __global__ void __launch_bounds__(128) k_conv_fwd_halo(const ConvFwdArgs a, int 
     if (warp == 0) tc::tmem_dealloc(tmem, ncols);
 }
 
-
-// ---------------------------------------------------------------------------
-// Weight gradient on the same halo tiles.  For one 16-channel input slice j
-// (blockIdx.x) and one range of output tiles (blockIdx.y):
-//
-//     D_tap[co][c] += sum over the tiles' voxels v of g[v][co] x[v + tap][c]
-//
-// one MMA per tap and 16 voxels: M = 128 output-channel rows (rows >= the
-// gradient's channels read zero planes), N = the 16 channels of the slice,
-// K = voxels.  Both operands are MN-major: the gradient tile as [8-channel
-// plane][voxel] x 16 bytes (core matrix = 8 consecutive voxels of a tile
-// row), the shifted input straight from the halo tile (8 consecutive halo x,
-// the next 8 voxels one halo row further).  The 27 taps' accumulators sit
-// side by side in tensor memory (27 x 16 of 512 columns) for the CTA's whole
-// range of tiles; at the end thread t writes row co = t of every tap into
-// the FP32 partial tile [split][k][nt] that k_wgrad_reduce sums.
-constexpr int GPLANE = 128 * 16;         // one 8-channel plane of a gradient tile
-constexpr int GTILE_BYTES = 16 * GPLANE; // 128 channel rows
-constexpr int WG_STAGES = 3;
-constexpr int WG_STAGE_BYTES = HALO_BYTES + GTILE_BYTES;
-constexpr int WG_SMEM_BYTES = WG_STAGES * WG_STAGE_BYTES + 8 * (WG_STAGES + 1) + 16;
-
-// Instruction descriptor: BF16 x BF16 -> FP32, A and B MN-major.
-__host__ __device__ constexpr uint32_t idesc_bf16_f32_mn(int M, int N) {
-    return tc::idesc_bf16_f32(M, N) | (1u << 15) | (1u << 16);
-}
-
-template <int NT>
-__global__ void __launch_bounds__(128) k_conv_wgrad_halo(const ConvWgradArgs a, int tiles,
-                                                         int tiles_per_split) {
-    extern __shared__ __align__(1024) uint8_t smem[];
-    constexpr int S = WG_STAGES, SB = WG_STAGE_BYTES;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + S * SB);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + S + 1);
-    const int tid = threadIdx.x, warp = tid >> 5;
-    constexpr uint32_t ncols = 512;
-    const uint32_t bar_acc = tc::smem_addr(&bars[S]);
-    auto bar_stage = [&](int s) { return tc::smem_addr(&bars[s]); };
-    const int j = blockIdx.x;  // input-channel slice
-    const int t0 = blockIdx.y * tiles_per_split;
-    const int nq = max(0, min(tiles, t0 + tiles_per_split) - t0);
-    const int gplanes = NT >> 3;  // planes of the gradient tile that are copied
-
-    // the gradient planes no copy writes stay zero (rows >= NT of every MMA)
-    if constexpr (NT < 128) {
-        constexpr int per = (16 - (NT >> 3)) * (GPLANE / 16);
-        for (int e = tid; e < S * per; e += 128) {
-            const int st = e / per, r = e - st * per;
-            *reinterpret_cast<uint4 *>(smem + st * SB + HALO_BYTES + gplanes * GPLANE + r * 16) =
-                make_uint4(0, 0, 0, 0);
-        }
-    }
-    tc::fence_async_smem();
-    if (warp == 0) {
-        tc::tmem_alloc(tc::smem_addr(tslot), ncols);
-        tc::tmem_relinquish();
-    }
-    if (tid == 0) {
-        for (int s = 0; s <= S; s++) tc::mbar_init(tc::smem_addr(&bars[s]), 1);
-        tc::mbar_init_fence();
-    }
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    const uint32_t tmem = *tslot;
-    constexpr uint32_t idesc = idesc_bf16_f32_mn(128, 16);
-
-    auto issue = [&](int q) {
-        const HaloTile t = halo_tile(a.d, t0 + q);
-        const uint32_t st_addr = tc::smem_addr(smem + (q % S) * SB);
-        for (int e = tid; e < 2 * HVOX; e += 128) {
-            const int kc = e >= HVOX, v = e - kc * HVOX;
-            const int hx = v % HX, hy = (v / HX) % HY, hz = v / (HX * HY);
-            const int gx = t.tx * 8 + hx - 1, gy = t.ty * 16 + hy - 1, gz = t.z + hz - 1;
-            const bool in = gx >= 0 && gx < a.d.nx && gy >= 0 && gy < a.d.ny && gz >= 0 &&
-                            gz < a.d.nz;
-            const long long vox =
-                in ? (((long long)t.b * a.d.nz + gz) * a.d.ny + gy) * a.d.nx + gx : 0;
-            cp_async16(st_addr + kc * HPLANE + v * 16,
-                       a.x + vox * a.x_stride + a.x_off + j * 16 + kc * 8, in ? 16u : 0u);
-        }
-        const uint32_t g_addr = st_addr + HALO_BYTES;
-        const long long v0 =
-            (((long long)t.b * a.d.nz + t.z) * a.d.ny + t.ty * 16) * a.d.nx + t.tx * 8;
-        for (int e = tid; e < gplanes * 128; e += 128) {
-            const int kc = e >> 7, v = e & 127;  // tile voxel v = x + 8 y
-            const long long vox = v0 + (long long)(v >> 3) * a.d.nx + (v & 7);
-            cp_async16(g_addr + kc * GPLANE + v * 16, a.g + vox * a.g_stride + kc * 8, 16u);
-        }
-    };
-
-    bool ok = true;
-    int last = -1;
-    for (int q = 0; q < S - 1; q++) {
-        if (q < nq) issue(q);
-        cp_async_commit();
-    }
-    for (int q = 0; q < nq; q++) {
-        const int s = q % S;
-        cp_async_wait<S - 2>();
-        tc::fence_async_smem();
-        tc::fence_before_sync();
-        __syncthreads();
-        tc::fence_after_sync();
-        if (tid == 0) {
-            const uint32_t hb = tc::smem_addr(smem + s * SB), gb = hb + HALO_BYTES;
-#pragma unroll 1
-            for (int tap = 0; tap < 27; tap++) {
-                const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
-#pragma unroll
-                for (int ks = 0; ks < 8; ks++) {  // tile rows 2 ks, 2 ks + 1
-                    const uint64_t ad = tc::kmajor_desc(gb + ks * 256, 128, GPLANE);
-                    const uint64_t bd = tc::kmajor_desc(
-                        hb + ((dz * HY + 2 * ks + dy) * HX + dx) * 16, HX * 16, HPLANE);
-                    tc::mma_bf16(tmem + (uint32_t)(tap * 16), ad, bd, idesc, (q | ks) != 0);
-                }
-            }
-            tc::mma_commit(bar_stage(s));
-            if (q == nq - 1) tc::mma_commit(bar_acc);
-        }
-        last = q;
-        const int qn = q + S - 1;
-        if (qn < nq) {
-            if (q >= 1) {
-                const bool got =
-                    tc::mbar_wait(bar_stage((q - 1) % S), ((q - 1) / S) & 1, WAIT_LIMIT);
-                if (!__syncthreads_and(got)) {
-                    ok = false;
-                    break;
-                }
-            }
-            issue(qn);
-        }
-        cp_async_commit();
-    }
-    if (ok && nq > 0) {
-        const bool got = tc::mbar_wait(bar_acc, 0, WAIT_LIMIT);
-        ok = __syncthreads_and(got) != 0;
-    }
-    bool drained = true;
-    if (!ok && last >= 0) {
-        bool got = tc::mbar_wait(bar_stage(last % S), (last / S) & 1, WAIT_LIMIT);
-        if (!__syncthreads_and(got)) {
-            got = tc::mbar_wait(bar_stage(last % S), (last / S) & 1, WAIT_LIMIT);
-            drained = __syncthreads_and(got) != 0;
-        }
-    }
-    tc::fence_after_sync();
-    // FP32 partials of this split: rows co < NT, k = tap * cin + 16 j + c
-    const int co = warp * 32 + (tid & 31);
-    float *out = a.partial + (long long)blockIdx.y * a.k_pad * NT;
-#pragma unroll 1
-    for (int tap = 0; tap < 27 && ok; tap++) {
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            float v[8];
-            tc::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(tap * 16 + h * 8), v);
-            tc::tmem_wait_ld();
-            if (co < NT) {
-                const int k0 = tap * a.cin + j * 16 + h * 8;
-#pragma unroll
-                for (int i = 0; i < 8; i++)
-                    out[(long long)(k0 + i) * NT + co] = nq > 0 ? v[i] : 0.f;
-            }
-        }
-    }
-    cp_async_wait_all();
-    if (!ok && tid == 0) atomicOr(a.err, drained ? 1 : 3);
-    tc::fence_before_sync();
-    __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, ncols);
-}
 
 }  // namespace nn
 }  // namespace lbm

@@ -225,15 +225,17 @@ __global__ void k_bias_grad_part(const __nv_bfloat16 *__restrict__ g, int nt, lo
     }
 }
 
-// Bias gradient, pass 2: db[c] = sum over blocks of partial[b][c] (FP64,
-// fixed order).
+// Bias gradient, pass 2: db[c] = sum over blocks of partial[b][c] in FP64;
+// one warp per channel, lane l summing blocks l, l + 32, ... and the lanes
+// combined by a fixed shuffle tree (deterministic).
 __global__ void k_bias_grad_sum(const float *__restrict__ partial, int blocks, int nt, int cout,
                                 float *__restrict__ db) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (c >= cout) return;
     double t = 0.0;
-    for (int b = 0; b < blocks; b++) t += partial[(long long)b * nt + c];
-    db[c] = (float)t;
+    for (int b = lane; b < blocks; b += 32) t += partial[(long long)b * nt + c];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (lane == 0) db[c] = (float)t;
 }
 
 // sum of squares of the gradient (for global-norm clipping)
@@ -482,7 +484,7 @@ struct Wsplit {
 Wsplit wgrad_split(long long m, int kpad) {
     const long long tiles = kpad / 128;
     const long long max_chunks = (m + KC - 1) / KC;
-    long long splits = (1184 + tiles - 1) / tiles;
+    long long splits = (1184 + tiles - 1) / tiles;  // about eight CTAs per SM
     if (splits > max_chunks) splits = max_chunks;
     if (splits < 1) splits = 1;
     const int chunks = (int)((max_chunks + splits - 1) / splits);
@@ -661,13 +663,15 @@ bool backward(LBMWarmNet *n, const float *target_dev, int nb) {
         w.m = m;
         const Wsplit sp = wgrad_split(m, w.k_pad);
         w.chunks_per_split = sp.chunks;
-        if (!ok(n, conv_wgrad(w, nt, sp.splits, n->grad + n->woff[l], 0, s, kLayers[l].cout)))
+        bool bias_done = false;
+        if (!ok(n, conv_wgrad(w, nt, sp.splits, n->grad + n->woff[l], 0, s, kLayers[l].cout,
+                              n->grad + n->boff[l], &bias_done)))
             return false;
-        {
+        if (!bias_done) {
             const unsigned bb = nblk(m, BG_ROWS);
             k_bias_grad_part<<<bb, 256, 0, s>>>(n->g, nt, m, n->bias_part);
-            k_bias_grad_sum<<<1, 256, 0, s>>>(n->bias_part, (int)bb, nt, kLayers[l].cout,
-                                              n->grad + n->boff[l]);
+            k_bias_grad_sum<<<(kLayers[l].cout + 7) / 8, 256, 0, s>>>(
+                n->bias_part, (int)bb, nt, kLayers[l].cout, n->grad + n->boff[l]);
         }
         if (!ok(n, cudaGetLastError())) return false;
         // input gradient

@@ -755,9 +755,9 @@ struct StepLaunch {
 
     static cudaError_t batch_pair(const BatchPairParams &p, int set, cudaStream_t s) {
         if constexpr (sizeof(typename S::T) <= 4) {
-            const unsigned tiles = p.starts[p.count];
-            if (p.count <= 0 || p.count > BATCH_LAUNCH_MAX || tiles == 0 || !p.grids)
+            if (p.count <= 0 || p.count > BATCH_LAUNCH_MAX || p.starts[p.count] == 0 || !p.grids)
                 return cudaErrorInvalidValue;
+            const unsigned tiles = p.starts[p.count];
             const dim3 blk(PAIR_THREADS);
             switch (set) {
                 case BATCH_SET_BGK: k_step_batch_pair<S, BATCH_SET_BGK><<<tiles, blk, 0, s>>>(p); break;

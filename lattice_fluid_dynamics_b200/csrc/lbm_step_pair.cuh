@@ -675,12 +675,13 @@ __global__ void __launch_bounds__(PAIR_THREADS, pair_minb<OP, SMAG>())
 // one fused step.  Work unit: one tile of one z-plane of one grid, one
 // PAIR_THREADS block per unit; the block finds its grid by binary search over
 // the unit offsets and copies that grid's entry (step arguments, operator,
-// tile shape) from the device table into shared memory, so nothing is
-// indexed at run time in the parameter space; the per-direction pointers
-// are computed from the buffers' bases (TabCalc) rather than read from the
-// entry's table, which would hold 57 pointers in registers.  The per-cell
+// tile shape; 160 bytes) from the device table into shared memory, so
+// nothing is indexed at run time in the parameter space; the per-direction
+// pointers are computed from the buffers' bases (TabCalc) rather than read
+// from a table, which would hold 57 pointers in registers.  The per-cell
 // code is k_step_pair's, so every grid's result is bit-identical to a solo
-// step.
+// step.  (Blocks that walk several units to share the set-up were measured
+// slower: the loop raised the spills.)
 template <class S, int SET>
 __global__ void __launch_bounds__(PAIR_THREADS, pair_minb_set(SET))
     k_step_batch_pair(const __grid_constant__ BatchPairParams p) {
@@ -709,7 +710,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, pair_minb_set(SET))
     const int y = ty * (PAIR_THREADS >> g.lbx) + (int)(threadIdx.x >> g.lbx);
     using T = typename S::T;
     const TabCalc<T> t{static_cast<const T *>(g.a.src), static_cast<T *>(g.a.dst), (int)g.a.n,
-                       g.a.nx, g.a.nx * g.a.ny, g.t.nz};
+                       g.a.nx, g.a.nx * g.a.ny, g.nz};
     constexpr unsigned M = batch_set_mask(SET);
     switch (g.combo) {
         case 0: if constexpr ((M & 1u) != 0) step_pair<S, OP_BGK, false, true>(g.a, t, x0, y, z); break;

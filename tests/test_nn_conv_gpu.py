@@ -178,7 +178,7 @@ def test_conv_forward_halo(solver, cin, cout, cout_pad, dims):
     ref = np.where(ref > 0, ref, 0.1 * ref)
     outs = {}
     try:
-        for path in (0, 1):
+        for path in (0, 1, 2):
             assert L.LBM_NNSetConvPath(path) == 0
             y = torch.full((m, ys), 7.0, dtype=torch.bfloat16, device="cuda")
             y32 = torch.full((m, ys), 7.0, dtype=torch.float32, device="cuda")
@@ -194,8 +194,9 @@ def test_conv_forward_halo(solver, cin, cout, cout_pad, dims):
             outs[path] = o32
     finally:
         L.LBM_NNSetConvPath(0)
-    # both kernels accumulate the same products in FP32, in different orders
+    # the kernels accumulate the same products in FP32, in different orders
     _close(outs[0][:, yo:yo + cout], outs[1][:, yo:yo + cout], 1e-5)
+    _close(outs[2][:, yo:yo + cout], outs[1][:, yo:yo + cout], 1e-5)
 
 
 @pytest.mark.gpu
@@ -228,9 +229,10 @@ def test_conv_input_gradient_halo(solver, cin, cout, cout_pad, dims):
 @pytest.mark.parametrize("cin,cout,cout_pad,dims",
                          [c for c in HALO_CASES if c[2] in (16, 32, 64)] +
                          [(16, 128, 128, (1, 2, 16, 8)), (32, 16, 16, (4, 8, 32, 16))])
-def test_conv_weight_gradient_halo(solver, cin, cout, cout_pad, dims):
-    """The halo-tiled weight gradient against the oracle and against the
-    gather kernel, with the input a channel slice of a wider buffer."""
+def test_conv_weight_gradient_paths(solver, cin, cout, cout_pad, dims):
+    """The weight gradient with MN-major operands (default) against the
+    oracle and against the gather kernel, with the input a channel slice of
+    a wider buffer."""
     L = capi.load()
     rng = np.random.default_rng(23 + cin + cout)
     m = int(np.prod(dims))
@@ -268,4 +270,4 @@ def test_nn_argument_checks_cpu():
                                1, 8, 8, 8, None) == 1
     assert L.LBM_NNConvWeightGrad(1, 8, 0, 8, 1, 16, 12, 16, 1, 0, 1, 1 << 30, 1,
                                   1, 8, 8, 8, None) == 1
-    assert L.LBM_NNSetConvPath(2) == 1 and L.LBM_NNSetConvPath(0) == 0
+    assert L.LBM_NNSetConvPath(3) == 1 and L.LBM_NNSetConvPath(0) == 0
