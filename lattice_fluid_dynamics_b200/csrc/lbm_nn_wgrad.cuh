@@ -81,7 +81,10 @@ __global__ void __launch_bounds__(128) k_conv_wgrad_mn(const ConvWgradArgs a) {
     // grp = (tid >> 6) + 2 i (i < 8), B channel groups n8 = (tid >> 6) + 2 i
     // (n8 < NT / 8).  Each A group's tap and channel offset, fixed for the CTA.
     const int j = tid & 63, g0 = tid >> 6;
+    // per group: tap offsets, the neighbour's voxel offset (valid when the
+    // neighbour is inside the grid: then it is voxel + toff) and channel
     int gdz[8], gdy[8], gdx[8], gch[8];
+    long long toff[8];
     bool gval[8], gone[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) {
@@ -93,7 +96,20 @@ __global__ void __launch_bounds__(128) k_conv_wgrad_mn(const ConvWgradArgs a) {
         gdz[i] = tap / 9 - 1;
         gdy[i] = (tap / 3) % 3 - 1;
         gdx[i] = tap % 3 - 1;
+        toff[i] = ((long long)gdz[i] * a.d.ny + gdy[i]) * a.d.nx + gdx[i];
     }
+    // coordinates of voxel vbase + j, advanced by KC voxels per chunk (32-bit:
+    // the launcher requires fewer than 2^31 voxels)
+    int cx, cy, cz;
+    {
+        unsigned r = (unsigned)min(vbase + j, a.m > 0 ? a.m - 1 : 0);
+        cx = (int)(r % (unsigned)a.d.nx);
+        r /= (unsigned)a.d.nx;
+        cy = (int)(r % (unsigned)a.d.ny);
+        r /= (unsigned)a.d.ny;
+        cz = (int)(r % (unsigned)a.d.nz);
+    }
+    int next_q = 0;  // chunk whose coordinates cx, cy, cz hold
 
     if (warp == 0) {
         tc::tmem_alloc(tc::smem_addr(tslot), ncols);
@@ -114,23 +130,27 @@ __global__ void __launch_bounds__(128) k_conv_wgrad_mn(const ConvWgradArgs a) {
         const uint32_t st = tc::smem_addr(smem + (q % S) * SB);
         const long long m = vbase + (long long)q * KC + j;
         const bool mv = m < a.m;
-        // voxel coordinates in 32-bit arithmetic (the launcher requires
-        // fewer than 2^31 voxels)
-        unsigned r = mv ? (unsigned)m : 0u;
-        const int x = (int)(r % (unsigned)a.d.nx);
-        r /= (unsigned)a.d.nx;
-        const int y = (int)(r % (unsigned)a.d.ny);
-        r /= (unsigned)a.d.ny;
-        const int z = (int)(r % (unsigned)a.d.nz);
-        const int b = (int)(r / (unsigned)a.d.nz);
+        // chunks are issued in order: step the coordinates by KC voxels per
+        // chunk (x wraps into y, y into z, z into the sample)
+        for (; next_q < q; next_q++) {
+            cx += KC;
+            while (cx >= a.d.nx) {
+                cx -= a.d.nx;
+                if (++cy == a.d.ny) {
+                    cy = 0;
+                    if (++cz == a.d.nz) cz = 0;
+                }
+            }
+        }
+        const int x = cx, y = cy, z = cz;
         // core-matrix offset of voxel j inside a row group: block j / 8, row j % 8
         const uint32_t voff = (uint32_t)((j >> 3) * 128 + (j & 7) * 16);
 #pragma unroll
         for (int i = 0; i < 8; i++) {
-            const int zz = z + gdz[i], yy = y + gdy[i], xx = x + gdx[i];
-            const bool in = mv && gval[i] && zz >= 0 && zz < a.d.nz && yy >= 0 && yy < a.d.ny &&
-                            xx >= 0 && xx < a.d.nx;
-            const long long nb = in ? (((long long)b * a.d.nz + zz) * a.d.ny + yy) * a.d.nx + xx : 0;
+            const bool in = mv && gval[i] && (unsigned)(z + gdz[i]) < (unsigned)a.d.nz &&
+                            (unsigned)(y + gdy[i]) < (unsigned)a.d.ny &&
+                            (unsigned)(x + gdx[i]) < (unsigned)a.d.nx;
+            const long long nb = in ? m + toff[i] : 0;
             if (gone[i])
                 cp_async16(st + (uint32_t)((g0 + 2 * i) * 1024) + voff, g_bf16_ones,
                            mv ? 16u : 0u);
@@ -271,8 +291,20 @@ __global__ void __launch_bounds__(128) k_conv_fwd_async(const ConvFwdArgs a) {
     const int vy = (int)(r % (unsigned)a.d.ny);
     r /= (unsigned)a.d.ny;
     const int vz = (int)(r % (unsigned)a.d.nz);
-    const int vb = (int)(r / (unsigned)a.d.nz);
     const uint32_t row_off = (uint32_t)((tid >> 3) * 1024 + (tid & 7) * 16);
+    // which of the 27 neighbours of row tid's voxel are inside the grid
+    unsigned nbmask = 0;
+    if (rv) {
+#pragma unroll
+        for (int tap = 0; tap < 27; tap++) {
+            const int zz = vz + tap / 9 - 1, yy = vy + (tap / 3) % 3 - 1, xx = vx + tap % 3 - 1;
+            if ((unsigned)zz < (unsigned)a.d.nz && (unsigned)yy < (unsigned)a.d.ny &&
+                (unsigned)xx < (unsigned)a.d.nx)
+                nbmask |= 1u << tap;
+        }
+    }
+    // k / cin as a multiply-high: exact for k * cin < 2^32 (k < 2^13 here)
+    const unsigned cin_magic = 0xFFFFFFFFu / (unsigned)a.cin + 1u;
 
     if (warp == 0) {
         tc::tmem_alloc(tc::smem_addr(tslot), ncols);
@@ -295,13 +327,12 @@ __global__ void __launch_bounds__(128) k_conv_fwd_async(const ConvFwdArgs a) {
         for (int g = 0; g < 8; g++) {
             const int k = kb + g * 8;
             const bool kv = k < a.k_real;
-            const int tap = kv ? k / a.cin : 0;
+            const int tap = kv ? (int)__umulhi((unsigned)k, cin_magic) : 0;
             const int ch = kv ? k - tap * a.cin : 0;
-            const int zz = vz + tap / 9 - 1, yy = vy + (tap / 3) % 3 - 1, xx = vx + tap % 3 - 1;
-            const bool in = rv && kv && (unsigned)zz < (unsigned)a.d.nz &&
-                            (unsigned)yy < (unsigned)a.d.ny && (unsigned)xx < (unsigned)a.d.nx;
-            const long long nb =
-                in ? (((long long)vb * a.d.nz + zz) * a.d.ny + yy) * a.d.nx + xx : 0;
+            const bool in = kv && ((nbmask >> tap) & 1u);
+            const long long toff =
+                ((long long)(tap / 9 - 1) * a.d.ny + ((tap / 3) % 3 - 1)) * a.d.nx + (tap % 3 - 1);
+            const long long nb = in ? mrow + toff : 0;
             cp_async16(st + row_off + (uint32_t)(g * 128),
                        a.x + nb * a.x_stride + a.x_off + ch, in ? 16u : 0u);
         }

@@ -423,6 +423,68 @@ def bench_train(steps: int, batch: int = 8, dims=(64, 32, 32)) -> dict:
             "gflop_per_step": flops / 1e9, "tflops": flops / (ms * 1e-3) / 1e12}
 
 
+# (cin, cout, dims (nb, nz, ny, nx)) of the convolutions bench_conv times:
+# the network's shapes at batch 8 and a 64x32x32 input
+CONV_SHAPES = [(16, 16, (8, 32, 32, 64)), (48, 16, (8, 32, 32, 64)), (8, 16, (8, 32, 32, 64)),
+               (16, 32, (8, 16, 16, 32)), (96, 32, (8, 16, 16, 32)),
+               (192, 64, (8, 8, 8, 16)), (64, 128, (8, 4, 4, 8))]
+
+
+def bench_conv(reps: int, ops=("fwd", "wgrad"), paths=(0, 1, 2)) -> list:
+    """Time LBM_NNConvForward / LBM_NNConvWeightGrad at the network's
+    shapes (CONV_SHAPES) through the C ABI with CUDA events, `reps` calls
+    after one untimed call, for each kernel path of LBM_NNSetConvPath
+    (0: halo / pipelined, 1: synchronous gather, 2: pipelined gather).
+    Random BF16 data; one dict per (shape, op, path)."""
+    import torch
+    L = capi.load()
+    out = []
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        b.synchronize()
+        return a.elapsed_time(b) / reps * 1e3
+
+    try:
+        for cin, cout, dims in CONV_SHAPES:
+            m = int(np.prod(dims))
+            nt = max(16, cout)
+            x = torch.randn(m, cin, device="cuda").to(torch.bfloat16)
+            w = (torch.randn(nt, L.LBM_NNKPad(cin), device="cuda") * 0.05).to(torch.bfloat16)
+            y = torch.zeros(m, nt, device="cuda", dtype=torch.bfloat16)
+            g = torch.randn(m, nt, device="cuda").to(torch.bfloat16)
+            wsb = L.LBM_NNWgradWorkspaceBytes(cin, nt, *dims, 8)
+            ws = torch.zeros(wsb // 4, device="cuda")
+            dw = torch.zeros(nt, 27 * cin, device="cuda")
+            flops = 2.0 * m * 27 * cin * cout
+            calls = {
+                "fwd": lambda: L.LBM_NNConvForward(x.data_ptr(), cin, 0, cin, w.data_ptr(), None,
+                                                   nt, 1, y.data_ptr(), None, nt, 0, nt, 0,
+                                                   *dims, None),
+                "wgrad": lambda: L.LBM_NNConvWeightGrad(x.data_ptr(), cin, 0, cin, g.data_ptr(),
+                                                        nt, nt, nt, dw.data_ptr(), 0,
+                                                        ws.data_ptr(), wsb, 8, *dims, None),
+            }
+            for path in paths:
+                L.LBM_NNSetConvPath(path)
+                for op in ops:
+                    us = timed(calls[op])
+                    out.append({"op": op, "path": path, "cin": cin, "cout": cout,
+                                "dims": list(dims), "us": round(us, 1),
+                                "tflops": round(flops / us / 1e6, 1)})
+    finally:
+        L.LBM_NNSetConvPath(0)
+    if L.LBM_NNTakeError() != 0:
+        raise RuntimeError("a convolution kernel gave up waiting for its tensor-core work")
+    return out
+
+
 # (cin, cout, level) of the 16 convolutions
 _LAYERS = [(8, 16, 0), (16, 16, 0), (16, 32, 1), (32, 32, 1), (32, 64, 2), (64, 64, 2),
            (64, 128, 3), (128, 128, 3), (128, 128, 3), (192, 64, 2), (64, 64, 2), (96, 32, 1),
@@ -455,12 +517,21 @@ def main(argv=None) -> int:
     ap.add_argument("--scaling", default="", help="results .json holding the output scaling")
     ap.add_argument("--bench-train", type=int, default=0,
                     help="only time this many training steps on synthetic data")
+    ap.add_argument("--bench-conv", type=int, default=0,
+                    help="only time the convolution kernels at the network's shapes (calls)")
+    ap.add_argument("--conv-op", default="fwd,wgrad", help="--bench-conv: fwd and / or wgrad")
+    ap.add_argument("--conv-path", default="0,1,2", help="--bench-conv: kernel paths")
     ap.add_argument("--fp16-reference", action="store_true",
                     help="also measure FP16 variants against a cold FP16 run's converged Cd")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     if a.bench_train:
         print(json.dumps(bench_train(a.bench_train, a.batch)))
+        return 0
+    if a.bench_conv:
+        for row in bench_conv(a.bench_conv, tuple(a.conv_op.split(",")),
+                              tuple(int(v) for v in a.conv_path.split(","))):
+            print(json.dumps(row), flush=True)
         return 0
     full = tuple(int(v) for v in a.grid.split("x"))
     half = tuple(v // 2 for v in full)
