@@ -13,6 +13,7 @@
 #include "lbm_nn_gemm.cuh"
 #include "lbm_nn_halo.cuh"
 #include "lbm_nn_wgrad.cuh"
+#include "lbm_nn_wgrad_halo.cuh"
 
 namespace lbm {
 namespace nn {
@@ -196,6 +197,49 @@ cudaError_t launch_fwd_gather(const ConvFwdArgs &a, dim3 grid, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+bool wgrad_halo_ok(const ConvWgradArgs &a, int nt) {
+    return g_conv_path == 0 && (nt == 16 || nt == 32) && a.cin % 16 == 0 &&
+           a.x_stride % 8 == 0 && a.x_off % 8 == 0 && a.g_stride % 8 == 0 && a.g_stride >= nt &&
+           a.d.nx % 8 == 0 && a.d.ny % 16 == 0 && a.m < (1ll << 31);
+}
+
+// Runs k_conv_wgrad_halo with at most `splits` tile ranges (the partial
+// workspace holds that many); returns the number used in *used.
+template <int NT>
+cudaError_t wgrad_halo_nt(const ConvWgradArgs &a, unsigned splits, unsigned *used,
+                          cudaStream_t s) {
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    static int sms = 0;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_conv_wgrad_halo<NT>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    wgh_smem_bytes<NT>());
+        if (attr == cudaSuccess)
+            attr = cudaFuncSetAttribute(k_conv_wgrad_halo<NT>,
+                                        cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        cudaSharedmemCarveoutMaxShared);
+        int dev = 0;
+        if (attr == cudaSuccess) attr = cudaGetDevice(&dev);
+        if (attr == cudaSuccess)
+            attr = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    });
+    if (attr != cudaSuccess) return attr;
+    const long long tiles = (long long)a.d.nb * a.d.nz * (a.d.ny / 16) * (a.d.nx / 8);
+    const int slices = a.cin / 16;
+    const int per_sm = NT <= 16 ? 2 : 1;  // shared memory: 108 / 117 KB per CTA
+    long long sp = ((long long)per_sm * sms + slices - 1) / slices;
+    if (sp > (long long)splits) sp = splits;
+    if (sp > tiles) sp = tiles;
+    if (sp < 1) sp = 1;
+    const long long per = (tiles + sp - 1) / sp;
+    sp = (tiles + per - 1) / per;
+    k_conv_wgrad_halo<NT><<<dim3(slices, (unsigned)sp), 128, wgh_smem_bytes<NT>(), s>>>(
+        a, (int)tiles, (int)per);
+    *used = (unsigned)sp;
+    return cudaGetLastError();
+}
+
 template <int NT>
 cudaError_t wgrad_mn_nt(const ConvWgradArgs &a, unsigned splits, cudaStream_t s) {
     static std::once_flag once;
@@ -300,7 +344,12 @@ cudaError_t conv_wgrad(const ConvWgradArgs &a0, int nt, unsigned splits, float *
     // the bias gradient rides on the first padding row group, if it exists
     a.ones_row = (mn && dbias && a.k_pad - a.k_real >= 8 && a.k_real % 8 == 0) ? a.k_real : -1;
     cudaError_t e;
-    if (mn) {
+    if (wgrad_halo_ok(a, nt)) {
+        unsigned used = splits;
+        e = nt == 16 ? wgrad_halo_nt<16>(a, splits, &used, s)
+                     : wgrad_halo_nt<32>(a, splits, &used, s);
+        splits = used;
+    } else if (mn) {
         switch (nt) {
             case 16: e = wgrad_mn_nt<16>(a, splits, s); break;
             case 32: e = wgrad_mn_nt<32>(a, splits, s); break;

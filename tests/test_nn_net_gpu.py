@@ -44,9 +44,11 @@ def test_param_count_matches_oracle(solver):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("nb", [1, 2])
-def test_forward_and_gradients_match_oracle(solver, nb):
-    dims = (nb,) + DIMS[1:]
+@pytest.mark.parametrize("nb,grid", [(1, DIMS[1:]), (2, DIMS[1:]), (1, (8, 16, 16))])
+def test_forward_and_gradients_match_oracle(solver, nb, grid):
+    """(8, 16, 16) runs the finest level on the halo-tiled kernels (NY a
+    multiple of 16), bias gradients folded into their weight gradients."""
+    dims = (nb,) + tuple(grid)
     net = capi.WarmNet(dims[3], dims[2], dims[1], max_batch=nb, seed=3)
     p = net.params()
     # give the output layer a larger scale so the prediction is not tiny
