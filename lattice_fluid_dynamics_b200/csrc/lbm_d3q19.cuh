@@ -102,6 +102,13 @@ struct StoreF64 {
         *reinterpret_cast<double2 *>(p) = make_double2(a, b);
     }
 };
+// paired IEEE add / subtract (defined below)
+__device__ __forceinline__ float2 padd(float2 a, float2 b);
+__device__ __forceinline__ float2 psub(float2 a, float2 b);
+
+// The 16-bit formats store f_i - w_i.  load2 / store2 move two neighbouring
+// cells with one packed conversion and one paired add / subtract: the same
+// roundings as two scalar loads / stores.
 struct StoreF16 {
     using T = __half;
     using R = float;
@@ -116,12 +123,13 @@ struct StoreF16 {
     }
     static __device__ __forceinline__ void load2(const T *p, int i, R &a, R &b) {
         const __half2 v = __ldg(reinterpret_cast<const __half2 *>(p));
-        a = __low2float(v) + wgt<float>(i);
-        b = __high2float(v) + wgt<float>(i);
+        const float2 r = padd(__half22float2(v), make_float2(wgt<float>(i), wgt<float>(i)));
+        a = r.x;
+        b = r.y;
     }
     static __device__ __forceinline__ void store2(T *p, R a, R b, int i) {
-        *reinterpret_cast<__half2 *>(p) =
-            __halves2half2(__float2half_rn(a - wgt<float>(i)), __float2half_rn(b - wgt<float>(i)));
+        const float2 d = psub(make_float2(a, b), make_float2(wgt<float>(i), wgt<float>(i)));
+        *reinterpret_cast<__half2 *>(p) = __floats2half2_rn(d.x, d.y);
     }
 };
 struct StoreBF16 {
@@ -138,12 +146,13 @@ struct StoreBF16 {
     }
     static __device__ __forceinline__ void load2(const T *p, int i, R &a, R &b) {
         const __nv_bfloat162 v = __ldg(reinterpret_cast<const __nv_bfloat162 *>(p));
-        a = __low2float(v) + wgt<float>(i);
-        b = __high2float(v) + wgt<float>(i);
+        const float2 r = padd(__bfloat1622float2(v), make_float2(wgt<float>(i), wgt<float>(i)));
+        a = r.x;
+        b = r.y;
     }
     static __device__ __forceinline__ void store2(T *p, R a, R b, int i) {
-        *reinterpret_cast<__nv_bfloat162 *>(p) = __halves2bfloat162(
-            __float2bfloat16_rn(a - wgt<float>(i)), __float2bfloat16_rn(b - wgt<float>(i)));
+        const float2 d = psub(make_float2(a, b), make_float2(wgt<float>(i), wgt<float>(i)));
+        *reinterpret_cast<__nv_bfloat162 *>(p) = __floats2bfloat162_rn(d.x, d.y);
     }
 };
 

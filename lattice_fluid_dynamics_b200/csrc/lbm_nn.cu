@@ -162,9 +162,14 @@ cudaError_t fwd_halo_nt(ConvFwdArgs a, cudaStream_t s) {
         if (attr == cudaSuccess) attr = cudaGetDevice(&dev);
         if (attr == cudaSuccess)
             attr = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        // CTAs per SM by shared memory (1 KB reserved per CTA); registers
+        // and threads allow more
+        int smem_sm = 0;
         if (attr == cudaSuccess)
-            attr = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv_fwd_halo<NT>, 128,
-                                                                 halo_smem_bytes<NT>());
+            attr = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor,
+                                          dev);
+        per_sm = smem_sm / (halo_smem_bytes<NT>() + 1024);
+        if (per_sm > 4) per_sm = 4;
         if (attr == cudaSuccess && per_sm < 1) attr = cudaErrorInvalidConfiguration;
     });
     if (attr != cudaSuccess) return attr;
