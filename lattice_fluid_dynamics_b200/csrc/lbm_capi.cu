@@ -60,7 +60,8 @@ size_t elem_size(int storage) {
 // blocks of 32 x 8 cells (a warp spans 32 consecutive x), at least 4 blocks
 // resident per SM (<= 64 registers), measured on B200 at 256x128x128 against
 // 64x4 / 128x2 / 256x1 shapes and an unconstrained register budget.
-// LBM_BLOCK=<bx>x<by>, LBM_MINB=1|4 and LBM_CPT=1|2 override it.
+// LBM_BLOCK=<bx>x<by>, LBM_MINB=1|4, LBM_CPT=1|2 and LBM_PBX=32|64|128
+// (threads along x of a paired block) override it.
 void default_block(GridImpl &I) {
     I.bx = 32;
     I.by = 8;
@@ -69,6 +70,11 @@ void default_block(GridImpl &I) {
     I.minb = 4;
     const char *cenv = getenv("LBM_CPT");
     if (cenv) I.cpt = atoi(cenv) == 2 ? 2 : 1;
+    const char *penv = getenv("LBM_PBX");
+    if (penv) {
+        const int v = atoi(penv);
+        if (v == 32 || v == 64 || v == 128) I.pbx = v;
+    }
     const char *menv = getenv("LBM_MINB");
     if (menv) I.minb = atoi(menv) == 1 ? 1 : 4;
     const char *env = getenv("LBM_BLOCK");

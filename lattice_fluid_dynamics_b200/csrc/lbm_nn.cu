@@ -273,16 +273,20 @@ cudaError_t wgrad_nt(ConvWgradArgs a, int slot, unsigned splits, cudaStream_t s)
 }
 
 
-// dW[n][k] = sum over splits of partial[split][k][n], n < cout, k < k_real.
-// Eight threads per output: thread r sums splits r, r + 8, ... and the
-// eight are combined by a fixed shuffle tree (deterministic); consecutive
-// outputs are consecutive n, so a warp reads contiguous partials.
+// dW[n][k] = sum over splits of partial[split][k][n], n < cout, k < k_real;
+// with dbias set, row k_real of the partials (the rows of 1.0 in the
+// reduction) summed the same way gives db[n].  Eight threads per output:
+// thread r sums splits r, r + 8, ... and the eight are combined by a fixed
+// shuffle tree (deterministic); consecutive outputs are consecutive n, so a
+// warp reads contiguous partials.
 __global__ void k_wgrad_reduce(const float *__restrict__ partial, int splits, int k_pad, int nt,
-                               int cout, int k_real, float *__restrict__ dw, int accumulate) {
+                               int cout, int k_real, float *__restrict__ dw, int accumulate,
+                               float *__restrict__ dbias) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int r = (int)(t & 7);
     const long long i = t >> 3;  // output index k * cout + n
-    const bool live = i < (long long)cout * k_real;
+    const int rows = k_real + (dbias ? 1 : 0);
+    const bool live = i < (long long)cout * rows;
     const int k = live ? (int)(i / cout) : 0, n = live ? (int)(i - (long long)k * cout) : 0;
     float s = 0.f;
     if (live)
@@ -291,8 +295,12 @@ __global__ void k_wgrad_reduce(const float *__restrict__ partial, int splits, in
     s += __shfl_down_sync(0xffffffffu, s, 2, 8);
     s += __shfl_down_sync(0xffffffffu, s, 1, 8);
     if (live && r == 0) {
-        float *o = dw + (long long)n * k_real + k;
-        *o = accumulate ? *o + s : s;
+        if (k == k_real) {
+            dbias[n] = s;
+        } else {
+            float *o = dw + (long long)n * k_real + k;
+            *o = accumulate ? *o + s : s;
+        }
     }
 }
 
@@ -373,16 +381,11 @@ cudaError_t conv_wgrad(const ConvWgradArgs &a0, int nt, unsigned splits, float *
     }
     if (e != cudaSuccess) return e;
     const int rows = cout_write > 0 ? cout_write : a.cout;
-    const long long total = 8ll * rows * a.k_real;
+    float *db = a.ones_row >= 0 ? dbias : nullptr;  // ones_row == k_real
+    const long long total = 8ll * rows * (a.k_real + (db ? 1 : 0));
     k_wgrad_reduce<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(
-        a.partial, (int)splits, a.k_pad, nt, rows, a.k_real, dw, accumulate);
-    if (a.ones_row >= 0) {
-        // db[n] = sum over splits of partial[split][ones_row][n]: the same
-        // reduction as one more row of dW, written to a [rows][1] matrix
-        k_wgrad_reduce<<<(unsigned)((8 * rows + 255) / 256), 256, 0, s>>>(
-            a.partial + (long long)a.ones_row * nt, (int)splits, a.k_pad, nt, rows, 1, dbias, 0);
-        if (bias_done) *bias_done = true;
-    }
+        a.partial, (int)splits, a.k_pad, nt, rows, a.k_real, dw, accumulate, db);
+    if (db && bias_done) *bias_done = true;
     return cudaGetLastError();
 }
 
