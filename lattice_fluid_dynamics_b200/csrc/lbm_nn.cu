@@ -275,31 +275,32 @@ cudaError_t wgrad_nt(ConvWgradArgs a, int slot, unsigned splits, cudaStream_t s)
 
 // dW[n][k] = sum over splits of partial[split][k][n], n < cout, k < k_real;
 // with dbias set, row k_real of the partials (the rows of 1.0 in the
-// reduction) summed the same way gives db[n].  Eight threads per output:
-// thread r sums splits r, r + 8, ... and the eight are combined by a fixed
-// shuffle tree (deterministic); consecutive outputs are consecutive n, so a
-// warp reads contiguous partials.
+// reduction) summed the same way gives db[n].  A block of 256 threads owns
+// 64 consecutive outputs o = k * cout + n (consecutive in the partials when
+// cout == nt, so a warp's loads are contiguous); thread group r (4 of them)
+// sums splits r, r + 4, ... and the four sums are added in order
+// (deterministic).
 __global__ void k_wgrad_reduce(const float *__restrict__ partial, int splits, int k_pad, int nt,
                                int cout, int k_real, float *__restrict__ dw, int accumulate,
                                float *__restrict__ dbias) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int r = (int)(t & 7);
-    const long long i = t >> 3;  // output index k * cout + n
+    __shared__ float part[4][64];
+    const int ol = threadIdx.x & 63, r = threadIdx.x >> 6;
+    const long long o = (long long)blockIdx.x * 64 + ol;
     const int rows = k_real + (dbias ? 1 : 0);
-    const bool live = i < (long long)cout * rows;
-    const int k = live ? (int)(i / cout) : 0, n = live ? (int)(i - (long long)k * cout) : 0;
+    const bool live = o < (long long)cout * rows;
+    const int k = live ? (int)(o / cout) : 0, n = live ? (int)(o - (long long)k * cout) : 0;
     float s = 0.f;
     if (live)
-        for (int p = r; p < splits; p += 8) s += partial[((long long)p * k_pad + k) * nt + n];
-    s += __shfl_down_sync(0xffffffffu, s, 4, 8);
-    s += __shfl_down_sync(0xffffffffu, s, 2, 8);
-    s += __shfl_down_sync(0xffffffffu, s, 1, 8);
-    if (live && r == 0) {
+        for (int p = r; p < splits; p += 4) s += partial[((long long)p * k_pad + k) * nt + n];
+    part[r][ol] = s;
+    __syncthreads();
+    if (r == 0 && live) {
+        const float t = ((part[0][ol] + part[1][ol]) + part[2][ol]) + part[3][ol];
         if (k == k_real) {
-            dbias[n] = s;
+            dbias[n] = t;
         } else {
-            float *o = dw + (long long)n * k_real + k;
-            *o = accumulate ? *o + s : s;
+            float *d = dw + (long long)n * k_real + k;
+            *d = accumulate ? *d + t : t;
         }
     }
 }
@@ -382,8 +383,8 @@ cudaError_t conv_wgrad(const ConvWgradArgs &a0, int nt, unsigned splits, float *
     if (e != cudaSuccess) return e;
     const int rows = cout_write > 0 ? cout_write : a.cout;
     float *db = a.ones_row >= 0 ? dbias : nullptr;  // ones_row == k_real
-    const long long total = 8ll * rows * (a.k_real + (db ? 1 : 0));
-    k_wgrad_reduce<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(
+    const long long outs = (long long)rows * (a.k_real + (db ? 1 : 0));
+    k_wgrad_reduce<<<(unsigned)((outs + 63) / 64), 256, 0, s>>>(
         a.partial, (int)splits, a.k_pad, nt, rows, a.k_real, dw, accumulate, db);
     if (db && bias_done) *bias_done = true;
     return cudaGetLastError();

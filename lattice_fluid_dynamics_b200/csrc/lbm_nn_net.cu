@@ -160,6 +160,38 @@ __global__ void k_act_bwd(const float *__restrict__ dout, int ds, int dof,
     g[i] = __float2bfloat16_rn(r);
 }
 
+// k_act_bwd for 8 channels per thread: two float4 loads of the output
+// gradient, one 16-byte load of the activations and one 16-byte store
+// (strides and offsets multiples of 8, c a multiple of 8, fewer than 2^31
+// groups -- checked by the caller).
+__global__ void k_act_bwd8(const float *__restrict__ dout, int ds, int dof,
+                           const __nv_bfloat16 *__restrict__ out, int os, int oo, int c, int act,
+                           __nv_bfloat16 *__restrict__ g, int nt, unsigned groups) {
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= groups) return;
+    const unsigned gq = (unsigned)nt >> 3, v = t / gq;
+    const int ch0 = (int)(t - v * gq) * 8;
+    __align__(16) __nv_bfloat16 h[8];
+    if (ch0 < c) {
+        const float4 *dp = reinterpret_cast<const float4 *>(dout + (long long)v * ds + dof + ch0);
+        const float4 a = dp[0], b = dp[1];
+        float r[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        if (act) {
+            const uint4 q = *reinterpret_cast<const uint4 *>(out + (long long)v * os + oo + ch0);
+            const __nv_bfloat16 *o = reinterpret_cast<const __nv_bfloat16 *>(&q);
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+                if (!(__bfloat162float(o[i]) > 0.f)) r[i] *= 0.1f;
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i++) h[i] = __float2bfloat16_rn(r[i]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 8; i++) h[i] = __float2bfloat16_rn(0.f);
+    }
+    *reinterpret_cast<uint4 *>(g + (long long)v * nt + ch0) = *reinterpret_cast<const uint4 *>(h);
+}
+
 // loss and its gradient on the 4 output channels (prediction stride 16)
 // Loss gradient of every output channel (16 per voxel, 4 real) and the
 // squared error summed into *loss: a grid-stride loop, one FP64 atomic per
@@ -643,8 +675,15 @@ bool backward(LBMWarmNet *n, const float *target_dev, int nb) {
         const Io io = layer_io(*n, l);
         const Gio gi = layer_gio(*n, l);
         if (l < NLAYERS - 1) {
-            k_act_bwd<<<nblk(m * nt), 256, 0, s>>>(gi.dout, gi.ds, gi.dof, io.y, io.ys, io.yo,
-                                                   kLayers[l].cout, kLayers[l].act, n->g, nt, m);
+            const int c = kLayers[l].cout;
+            if (gi.ds % 4 == 0 && gi.dof % 4 == 0 && io.ys % 8 == 0 && io.yo % 8 == 0 &&
+                c % 8 == 0 && nt % 8 == 0 && m * (nt / 8) < (1ll << 31))
+                k_act_bwd8<<<nblk(m * (nt / 8)), 256, 0, s>>>(gi.dout, gi.ds, gi.dof, io.y, io.ys,
+                                                              io.yo, c, kLayers[l].act, n->g, nt,
+                                                              (unsigned)(m * (nt / 8)));
+            else
+                k_act_bwd<<<nblk(m * nt), 256, 0, s>>>(gi.dout, gi.ds, gi.dof, io.y, io.ys, io.yo,
+                                                       c, kLayers[l].act, n->g, nt, m);
             if (!ok(n, cudaGetLastError())) return false;
         }
         // weight and bias gradients
