@@ -277,25 +277,30 @@ cudaError_t wgrad_nt(ConvWgradArgs a, int slot, unsigned splits, cudaStream_t s)
 // with dbias set, row k_real of the partials (the rows of 1.0 in the
 // reduction) summed the same way gives db[n].  A block of 256 threads owns
 // 64 consecutive outputs o = k * cout + n (consecutive in the partials when
-// cout == nt, so a warp's loads are contiguous); thread group r (4 of them)
-// sums splits r, r + 4, ... and the four sums are added in order
-// (deterministic).
+// cout == nt, so each warp's loads are one contiguous 128-byte line); thread
+// group r (4 of them, two warps each) sums splits r, r + 4, ... and the four
+// sums are added in order (deterministic).  (Measured: 4 x 64 outputs per
+// block faster than 8 x 32 and 16 x 16.)
+constexpr int WR_OUT = 64, WR_GROUPS = 4;
 __global__ void k_wgrad_reduce(const float *__restrict__ partial, int splits, int k_pad, int nt,
                                int cout, int k_real, float *__restrict__ dw, int accumulate,
                                float *__restrict__ dbias) {
-    __shared__ float part[4][64];
-    const int ol = threadIdx.x & 63, r = threadIdx.x >> 6;
-    const long long o = (long long)blockIdx.x * 64 + ol;
+    __shared__ float part[WR_GROUPS][WR_OUT];
+    const int ol = threadIdx.x % WR_OUT, r = threadIdx.x / WR_OUT;
+    const long long o = (long long)blockIdx.x * WR_OUT + ol;
     const int rows = k_real + (dbias ? 1 : 0);
     const bool live = o < (long long)cout * rows;
     const int k = live ? (int)(o / cout) : 0, n = live ? (int)(o - (long long)k * cout) : 0;
     float s = 0.f;
     if (live)
-        for (int p = r; p < splits; p += 4) s += partial[((long long)p * k_pad + k) * nt + n];
+        for (int p = r; p < splits; p += WR_GROUPS)
+            s += partial[((long long)p * k_pad + k) * nt + n];
     part[r][ol] = s;
     __syncthreads();
     if (r == 0 && live) {
-        const float t = ((part[0][ol] + part[1][ol]) + part[2][ol]) + part[3][ol];
+        float t = part[0][ol];
+#pragma unroll
+        for (int q = 1; q < WR_GROUPS; q++) t += part[q][ol];
         if (k == k_real) {
             dbias[n] = t;
         } else {
@@ -384,7 +389,7 @@ cudaError_t conv_wgrad(const ConvWgradArgs &a0, int nt, unsigned splits, float *
     const int rows = cout_write > 0 ? cout_write : a.cout;
     float *db = a.ones_row >= 0 ? dbias : nullptr;  // ones_row == k_real
     const long long outs = (long long)rows * (a.k_real + (db ? 1 : 0));
-    k_wgrad_reduce<<<(unsigned)((outs + 63) / 64), 256, 0, s>>>(
+    k_wgrad_reduce<<<(unsigned)((outs + WR_OUT - 1) / WR_OUT), WR_OUT * WR_GROUPS, 0, s>>>(
         a.partial, (int)splits, a.k_pad, nt, rows, a.k_real, dw, accumulate, db);
     if (db && bias_done) *bias_done = true;
     return cudaGetLastError();

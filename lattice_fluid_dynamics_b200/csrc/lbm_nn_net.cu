@@ -298,15 +298,52 @@ __global__ void k_adam(float *__restrict__ p, const float *__restrict__ g, float
     p[i] -= lr_t * mi / (sqrtf(vi) + eps);
 }
 
-// master weights -> BF16 [nt][k_pad] (zero padded) and FP32 bias [nt]
-__global__ void k_pack(const float *__restrict__ w, const float *__restrict__ b, int cout,
-                       int kreal, __nv_bfloat16 *__restrict__ wb, float *__restrict__ bias,
-                       int nt, int kpad) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nt) bias[i] = i < cout ? b[i] : 0.f;
-    if (i >= nt * kpad) return;
-    const int n = i / kpad, k = i - n * kpad;
-    wb[i] = __float2bfloat16_rn((n < cout && k < kreal) ? w[(long long)n * kreal + k] : 0.f);
+// All layers' packing in one launch: per layer the BF16 weights [nt][k_pad]
+// and FP32 bias [nt] of k_pack, and (layers > 0) the flipped, transposed
+// BF16 weights of the input gradient, wt[ci][(26 - tap) nt + co] =
+// bf16(W[co][tap cin + ci]) (zero for ci >= cin or co >= cout) -- the values
+// k_pack + k_weight_transpose produce, computed from the FP32 masters.
+struct PackLayer {
+    const float *w, *b;
+    __nv_bfloat16 *wb, *wt;
+    float *bias;
+    int cout, cin, nt, kpad, wt_rows, wt_kpad;
+    long long start;  // first element of this layer in the launch
+};
+struct PackTable {
+    PackLayer l[16];
+    long long total;
+};
+
+__global__ void k_pack_all(const __grid_constant__ PackTable t) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= t.total) return;
+    int l = 0;
+    while (l < 15 && i >= t.l[l + 1].start) l++;
+    const PackLayer &L = t.l[l];
+    long long e = i - L.start;
+    const int kreal = 27 * L.cin;
+    const long long nwb = (long long)L.nt * L.kpad;
+    if (e < nwb) {
+        const int n = (int)(e / L.kpad), k = (int)(e - (long long)n * L.kpad);
+        L.wb[e] = __float2bfloat16_rn((n < L.cout && k < kreal) ? L.w[(long long)n * kreal + k]
+                                                                 : 0.f);
+        return;
+    }
+    e -= nwb;
+    if (e < L.nt) {
+        L.bias[e] = e < L.cout ? L.b[e] : 0.f;
+        return;
+    }
+    e -= L.nt;
+    // transposed weights
+    const int ci = (int)(e / L.wt_kpad), k = (int)(e - (long long)ci * L.wt_kpad);
+    float v = 0.f;
+    if (ci < L.cin && k < 27 * L.nt) {
+        const int tp = k / L.nt, co = k - tp * L.nt;
+        if (co < L.cout) v = L.w[(long long)co * kreal + (26 - tp) * L.cin + ci];
+    }
+    L.wt[e] = __float2bfloat16_rn(v);
 }
 
 struct OutScale {
@@ -599,16 +636,28 @@ Gio layer_gio(const LBMWarmNet &n, int l) {
 }
 
 bool pack(LBMWarmNet *n) {
+    static_assert(NLAYERS == 16, "PackTable holds 16 layers");
+    PackTable t{};
+    long long at = 0;
     for (int l = 0; l < NLAYERS; l++) {
-        const int nt = nt_of(kLayers[l].cout), kp = k_pad_of(kLayers[l].cin);
-        k_pack<<<nblk((long long)nt * kp), 256, 0, n->stream>>>(
-            n->params + n->woff[l], n->params + n->boff[l], kLayers[l].cout,
-            27 * kLayers[l].cin, n->wb[l], n->bias[l], nt, kp);
-        if (!ok(n, cudaGetLastError())) return false;
-        if (l > 0 && !ok(n, weight_transpose(n->wb[l], nt, kLayers[l].cin, n->wt[l],
-                                             pad16(kLayers[l].cin), n->stream)))
-            return false;
+        PackLayer &L = t.l[l];
+        L.w = n->params + n->woff[l];
+        L.b = n->params + n->boff[l];
+        L.wb = n->wb[l];
+        L.wt = l > 0 ? n->wt[l] : nullptr;
+        L.bias = n->bias[l];
+        L.cout = kLayers[l].cout;
+        L.cin = kLayers[l].cin;
+        L.nt = nt_of(L.cout);
+        L.kpad = k_pad_of(L.cin);
+        L.wt_rows = l > 0 ? pad16(L.cin) : 0;
+        L.wt_kpad = k_pad_of(L.nt);
+        L.start = at;
+        at += (long long)L.nt * L.kpad + L.nt + (long long)L.wt_rows * L.wt_kpad;
     }
+    t.total = at;
+    k_pack_all<<<nblk(at), 256, 0, n->stream>>>(t);
+    if (!ok(n, cudaGetLastError())) return false;
     n->packed = true;
     return true;
 }
