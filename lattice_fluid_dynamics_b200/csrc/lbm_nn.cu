@@ -176,7 +176,7 @@ cudaError_t fwd_halo_nt(ConvFwdArgs a, cudaStream_t s) {
     const long long tiles = (long long)a.d.nb * a.d.nz * (a.d.ny / 16) * (a.d.nx / 8);
     const long long cap = (long long)per_sm * sms;
     const unsigned blocks = (unsigned)(tiles < cap ? tiles : cap);
-    k_conv_fwd_halo<NT><<<blocks, 128, halo_smem_bytes<NT>(), s>>>(a, (int)tiles);
+    k_conv_fwd_halo<NT><<<blocks, HALO_THREADS, halo_smem_bytes<NT>(), s>>>(a, (int)tiles);
     return cudaGetLastError();
 }
 
@@ -239,7 +239,7 @@ cudaError_t wgrad_halo_nt(const ConvWgradArgs &a, unsigned splits, unsigned *use
     if (sp < 1) sp = 1;
     const long long per = (tiles + sp - 1) / sp;
     sp = (tiles + per - 1) / per;
-    k_conv_wgrad_halo<NT><<<dim3(slices, (unsigned)sp), 128, wgh_smem_bytes<NT>(), s>>>(
+    k_conv_wgrad_halo<NT><<<dim3(slices, (unsigned)sp), WGH_THREADS, wgh_smem_bytes<NT>(), s>>>(
         a, (int)tiles, (int)per);
     *used = (unsigned)sp;
     return cudaGetLastError();

@@ -26,9 +26,10 @@
 // shared memory: every thread copies its share of item q + S - 1 while the
 // tensor core works on item q, one thread issues the 27 MMAs of an item and
 // commits them to the stage's mbarrier, and after the last slice of a tile
-// every thread reads its accumulator row from tensor memory (thread t: row
-// t) for the bias / activation / store epilogue.  CTAs are persistent over
-// tiles (tile = blockIdx.x + i * gridDim.x).
+// every thread reads its accumulator row from tensor memory for the bias /
+// activation / store epilogue (256 threads: warp w reads rows 32 (w % 4) ..
+// + 31, columns of half w / 4).  CTAs are persistent over tiles (tile =
+// blockIdx.x + i * gridDim.x).
 //
 // Every wait is bounded and block-uniform; when one gives up the CTA stops
 // issuing copies and MMAs, drains the MMAs it committed (bounded), sets the
@@ -98,8 +99,10 @@ __device__ __forceinline__ HaloTile halo_tile(const Dims &d, int tile) {
     return t;
 }
 
+constexpr int HALO_THREADS = 256;
+
 template <int NT>
-__global__ void __launch_bounds__(128) k_conv_fwd_halo(const ConvFwdArgs a, int tiles) {
+__global__ void __launch_bounds__(HALO_THREADS) k_conv_fwd_halo(const ConvFwdArgs a, int tiles) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int S = halo_stages<NT>(), SB = halo_stage_bytes<NT>();
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + S * SB);  // S stage barriers, 1 tile
@@ -127,16 +130,16 @@ __global__ void __launch_bounds__(128) k_conv_fwd_halo(const ConvFwdArgs a, int 
     const int my_tiles = (int)blockIdx.x < tiles ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     const int nq = my_tiles * ck;
 
-    // This thread's halo elements e = tid + 128 i: shared-memory offset,
+    // This thread's halo elements e = tid + 256 i: shared-memory offset,
     // position in the halo and voxel offset from the halo's (1, 1, 1) corner
     // -- the same for every tile.
-    constexpr int HE = (2 * HVOX + 127) / 128;
+    constexpr int HE = (2 * HVOX + HALO_THREADS - 1) / HALO_THREADS;
     uint32_t h_soff[HE];
     int h_pos[HE];   // hx | hy << 8 | hz << 16 | kc << 24, or -1 past the end
     int h_rel[HE];   // voxel offset
 #pragma unroll
     for (int i = 0; i < HE; i++) {
-        const int e = tid + 128 * i;
+        const int e = tid + HALO_THREADS * i;
         const int kc = e >= HVOX, v = e - kc * HVOX;
         const int hx = v % HX, hy = (v / HX) % HY, hz = v / (HX * HY);
         h_soff[i] = (uint32_t)(kc * HPLANE + v * 16);
@@ -167,7 +170,7 @@ __global__ void __launch_bounds__(128) k_conv_fwd_halo(const ConvFwdArgs a, int 
         }
         if (ck > 1 || q == 0) {
             const uint32_t w_addr = st_addr + HALO_BYTES;
-            for (int e = tid; e < 54 * NT; e += 128) {
+            for (int e = tid; e < 54 * NT; e += HALO_THREADS) {
                 const int n = e % NT, tk = e / NT;  // tk = tap * 2 + plane
                 cp_async16(w_addr + (tk * NT + n) * 16,
                            a.w + (long long)n * a.k_pad + (tk >> 1) * a.cin + j * 16 + (tk & 1) * 8,
@@ -233,14 +236,15 @@ __global__ void __launch_bounds__(128) k_conv_fwd_halo(const ConvFwdArgs a, int 
             tiles_done++;
             tc::fence_after_sync();
             const HaloTile t = halo_tile(a.d, (int)blockIdx.x + (q / ck) * (int)gridDim.x);
-            const int row = warp * 32 + (tid & 31);
+            const int row = (warp & 3) * 32 + (tid & 31);
             const long long m =
                 (((long long)t.b * a.d.nz + t.z) * a.d.ny + t.ty * 16 + (row >> 3)) * a.d.nx +
                 t.tx * 8 + (row & 7);
+            const int c0 = (warp >> 2) * (NT / 2);
 #pragma unroll 1
-            for (int col = 0; col < NT; col += 8) {
+            for (int col = c0; col < c0 + NT / 2; col += 8) {
                 float v[8];
-                tc::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)col, v);
+                tc::tmem_ld8(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)col, v);
                 tc::tmem_wait_ld();
                 fwd_store(a, m, col, v);
             }

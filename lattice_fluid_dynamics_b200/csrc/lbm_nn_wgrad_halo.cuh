@@ -11,9 +11,9 @@
 // Per tile the halo (as in the forward) and the gradient tile are copied by
 // cp.async; then for each row tile the A operand -- MN-major, [row group
 // (tap, 8 channels)][8-voxel block][voxel] x 16 bytes, the tile's im2col
-// transposed -- is built in shared memory from the halo (thread t copies
-// voxel t's 16 row groups: 16-byte shared loads and stores at compile-time
-// offsets) and one thread issues its 8 MMAs (M = 128, N = NT, K = 16
+// transposed -- is built in shared memory from the halo (256 threads: thread
+// t copies 8 of voxel t % 128's 16 row groups with 16-byte shared loads and
+// stores at compile-time offsets) and one thread issues its 8 MMAs (M = 128, N = NT, K = 16
 // voxels) against the gradient tile (MN-major [8-channel group][8-voxel
 // block][voxel]).  A is double-buffered, so the build of row tile t + 1
 // overlaps the MMAs of row tile t, and each voxel's data crosses L2 once per
@@ -48,9 +48,11 @@ __host__ __device__ constexpr int wgh_smem_bytes() {
     return 2 * wgh_stage_bytes<NT>() + 2 * WGH_A_BYTES + 8 * 5 + 16;
 }
 
+constexpr int WGH_THREADS = 256;
+
 template <int NT>
-__global__ void __launch_bounds__(128) k_conv_wgrad_halo(const ConvWgradArgs a, int tiles,
-                                                         int tiles_per_split) {
+__global__ void __launch_bounds__(WGH_THREADS) k_conv_wgrad_halo(const ConvWgradArgs a, int tiles,
+                                                                 int tiles_per_split) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int SB = wgh_stage_bytes<NT>();
     uint8_t *abuf = smem + 2 * SB;
@@ -65,22 +67,24 @@ __global__ void __launch_bounds__(128) k_conv_wgrad_halo(const ConvWgradArgs a, 
     const bool ones = a.ones_row >= 0 && j == 0;
 
     // per-thread halo copy offsets (as in the forward)
-    constexpr int HE = (2 * HVOX + 127) / 128;
+    constexpr int HE = (2 * HVOX + WGH_THREADS - 1) / WGH_THREADS;
     uint32_t h_soff[HE];
     int h_pos[HE], h_rel[HE];
 #pragma unroll
     for (int i = 0; i < HE; i++) {
-        const int e = tid + 128 * i;
+        const int e = tid + WGH_THREADS * i;
         const int kc = e >= HVOX, v = e - kc * HVOX;
         const int hx = v % HX, hy = (v / HX) % HY, hz = v / (HX * HY);
         h_soff[i] = (uint32_t)(kc * HPLANE + v * 16);
         h_pos[i] = e < 2 * HVOX ? (hx | hy << 8 | hz << 16 | kc << 24) : -1;
         h_rel[i] = ((hz - 1) * a.d.ny + (hy - 1)) * a.d.nx + (hx - 1);
     }
-    // thread t handles voxel t = (x, y) of the tile: its 16-byte slot in the
-    // MN-major layouts and its place in the halo (tap (0, 0, 0) corner)
-    const int vx = tid & 7, vy = tid >> 3;
-    const uint32_t a_voff = (uint32_t)((tid >> 3) * 128 + (tid & 7) * 16);
+    // thread t handles voxel t % 128 = (x, y) of the tile (its 16-byte slot
+    // in the MN-major layouts and its place in the halo, tap (0, 0, 0)
+    // corner) for half t / 128 of the row groups and gradient channels
+    const int vt = tid & 127, half = tid >> 7;
+    const int vx = vt & 7, vy = vt >> 3;
+    const uint32_t a_voff = (uint32_t)((vt >> 3) * 128 + (vt & 7) * 16);
     const uint32_t h_voff = (uint32_t)((vy * HX + vx) * 16);
 
     if (warp == 0) {
@@ -117,9 +121,11 @@ __global__ void __launch_bounds__(128) k_conv_wgrad_halo(const ConvWgradArgs a, 
         }
         const long long vox = base + (long long)vy * a.d.nx + vx;
 #pragma unroll
-        for (int n8 = 0; n8 < NT / 8; n8++)
+        for (int i = 0; i < NT / 16; i++) {
+            const int n8 = half + 2 * i;
             cp_async16(st + HALO_BYTES + (uint32_t)(n8 * 2048) + a_voff,
                        a.g + vox * a.g_stride + n8 * 8, n8 * 8 < a.cout ? 16u : 0u);
+        }
     };
 
     // all threads: row tile rt of the A operand from halo stage s into buffer b
@@ -127,7 +133,8 @@ __global__ void __launch_bounds__(128) k_conv_wgrad_halo(const ConvWgradArgs a, 
         const uint8_t *h = smem + s * SB + h_voff;
         uint8_t *dst = abuf + b * WGH_A_BYTES + a_voff;
 #pragma unroll
-        for (int gi = 0; gi < 16; gi++) {
+        for (int gh = 0; gh < 8; gh++) {
+            const int gi = half * 8 + gh;
             const int tap = 8 * rt + (gi >> 1), kc = gi & 1;
             uint4 v = make_uint4(0u, 0u, 0u, 0u);
             if (tap < 27) {
@@ -212,18 +219,20 @@ __global__ void __launch_bounds__(128) k_conv_wgrad_halo(const ConvWgradArgs a, 
     }
     tc::fence_after_sync();
     if (ok) {
-        // row r = 32 warp + lane of each row tile: group r / 8, channel r % 8
-        const int r = warp * 32 + (tid & 31), gi = r >> 3;
+        // row r = 32 (warp % 4) + lane of row tiles 2 half, 2 half + 1:
+        // group r / 8, channel r % 8
+        const int r = (warp & 3) * 32 + (tid & 31), gi = r >> 3;
         float *out = a.partial + (long long)blockIdx.y * a.k_pad * NT;
 #pragma unroll 1
-        for (int rt = 0; rt < 4; rt++) {
+        for (int rt = 2 * half; rt < 2 * half + 2; rt++) {
             const int tap = 8 * rt + (gi >> 1), c = (gi & 1) * 8 + (r & 7);
             const bool keep = tap < 27 || (tap == 27 && (gi & 1) == 0 && ones);
             float *row = out + (long long)(tap * a.cin + j * 16 + c) * NT;
 #pragma unroll
             for (int col = 0; col < NT; col += 8) {
                 float v[8];
-                tc::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(rt * NT + col), v);
+                tc::tmem_ld8(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(rt * NT + col),
+                             v);
                 tc::tmem_wait_ld();
                 if (nq == 0) {
 #pragma unroll
