@@ -387,8 +387,11 @@ int LBM_NNTakeError(void);
  * a multiple of 16, coutPad 16 / 32 / 48 / 64 / 96) and the cp.async-
  * pipelined im2col kernels elsewhere (and for every weight gradient); 1 the
  * original synchronous im2col kernels for every shape; 2 the pipelined
- * im2col kernels for every shape.  Process-wide; not thread-safe against
- * concurrent launches.  LBM_OK or LBM_ERR_INVALID_ARGUMENT. */
+ * im2col kernels for every shape; 3 as 0 with the z-folded forward (three
+ * z taps per MMA, coutPad 16 / 32) wherever the shape allows it, also where
+ * 0 would not choose it for lack of parallelism.  Process-wide; not
+ * thread-safe against concurrent launches.  LBM_OK or
+ * LBM_ERR_INVALID_ARGUMENT. */
 int LBM_NNSetConvPath(int path);
 
 /* The warm-start network: a 4-level 3D conv encoder-decoder (8->16->32->64

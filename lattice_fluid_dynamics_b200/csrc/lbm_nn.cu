@@ -14,6 +14,7 @@
 #include "lbm_nn_halo.cuh"
 #include "lbm_nn_wgrad.cuh"
 #include "lbm_nn_wgrad_halo.cuh"
+#include "lbm_nn_zfold.cuh"
 
 namespace lbm {
 namespace nn {
@@ -135,15 +136,49 @@ cudaError_t fwd_nt(ConvFwdArgs a, int slot, cudaStream_t s) {
 // 0: the halo-tiled forward kernel where a convolution's shape allows it,
 //    the cp.async-pipelined gather kernels elsewhere;
 // 1: the original synchronous gather kernels for every shape;
-// 2: the pipelined gather kernels for every shape
+// 2: the pipelined gather kernels for every shape;
+// 3: as 0, with the z-folded forward wherever its shape allows it (not only
+//    where there are enough tile columns to fill the GPU)
 // (LBM_NNSetConvPath, for comparisons)
 int g_conv_path = 0;
 
 bool halo_shape_ok(const ConvFwdArgs &a, int nt) {
-    return g_conv_path == 0 && a.cin % 16 == 0 && a.x_stride % 8 == 0 && a.x_off % 8 == 0 &&
+    return (g_conv_path == 0 || g_conv_path == 3) && a.cin % 16 == 0 && a.x_stride % 8 == 0 && a.x_off % 8 == 0 &&
            a.d.nx % 8 == 0 && a.d.ny % 16 == 0 &&
            (nt == 16 || nt == 32 || nt == 48 || nt == 64 || nt == 96) &&
            (long long)a.d.nb * a.d.nz * (a.d.ny / 16) * (a.d.nx / 8) < (1ll << 31);
+}
+
+// The z-folded forward where there are enough columns of tiles to keep
+// every SM busy with ZF_SEG output planes per CTA and a single input slice
+// (its weights stay resident; with more slices the per-plane weight copies
+// cost more than the saved MMAs: 157 against 149 us for 48 -> 16 at
+// 8 x 64x32x32).  Path 3 takes it wherever the kernel can run.
+bool zfold_ok(const ConvFwdArgs &a, int nt) {
+    const long long cols = (long long)a.d.nb * (a.d.ny / 16) * (a.d.nx / 8);
+    const long long segs = (a.d.nz + ZF_SEG - 1) / ZF_SEG;
+    return (nt == 16 || nt == 32) && cols < (1ll << 31) &&
+           (g_conv_path == 3 || (a.cin == 16 && cols * segs >= 296));
+}
+
+template <int NT>
+cudaError_t fwd_zfold_nt(const ConvFwdArgs &a, cudaStream_t s) {
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_conv_fwd_zfold<NT>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    zf_smem_bytes<NT>());
+        if (attr == cudaSuccess)
+            attr = cudaFuncSetAttribute(k_conv_fwd_zfold<NT>,
+                                        cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        cudaSharedmemCarveoutMaxShared);
+    });
+    if (attr != cudaSuccess) return attr;
+    const unsigned cols = (unsigned)((long long)a.d.nb * (a.d.ny / 16) * (a.d.nx / 8));
+    const unsigned segs = (unsigned)((a.d.nz + ZF_SEG - 1) / ZF_SEG);
+    k_conv_fwd_zfold<NT><<<dim3(cols, segs), 128, zf_smem_bytes<NT>(), s>>>(a);
+    return cudaGetLastError();
 }
 
 template <int NT>
@@ -332,6 +367,7 @@ cudaError_t conv_forward(const ConvFwdArgs &a0, int nt, cudaStream_t s) {
     a.err = err_ptr();
     if (!a.err) return cudaErrorInvalidDevicePointer;
     if (halo_shape_ok(a, nt)) {
+        if (zfold_ok(a, nt)) return nt == 16 ? fwd_zfold_nt<16>(a, s) : fwd_zfold_nt<32>(a, s);
         switch (nt) {
             case 16: return fwd_halo_nt<16>(a, s);
             case 32: return fwd_halo_nt<32>(a, s);
@@ -505,7 +541,7 @@ int LBM_NNConvWeightGrad(const void *x, int xStride, int xOff, int cin, const vo
 int LBM_NNTakeError(void) { return take_error() ? LBM_ERR_TIMEOUT : LBM_OK; }
 
 int LBM_NNSetConvPath(int path) {
-    if (path < 0 || path > 2) return LBM_ERR_INVALID_ARGUMENT;
+    if (path < 0 || path > 3) return LBM_ERR_INVALID_ARGUMENT;
     g_conv_path = path;
     return LBM_OK;
 }

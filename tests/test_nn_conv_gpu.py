@@ -178,7 +178,7 @@ def test_conv_forward_halo(solver, cin, cout, cout_pad, dims):
     ref = np.where(ref > 0, ref, 0.1 * ref)
     outs = {}
     try:
-        for path in (0, 1, 2):
+        for path in (0, 1, 2, 3):
             assert L.LBM_NNSetConvPath(path) == 0
             y = torch.full((m, ys), 7.0, dtype=torch.bfloat16, device="cuda")
             y32 = torch.full((m, ys), 7.0, dtype=torch.float32, device="cuda")
@@ -197,6 +197,7 @@ def test_conv_forward_halo(solver, cin, cout, cout_pad, dims):
     # the kernels accumulate the same products in FP32, in different orders
     _close(outs[0][:, yo:yo + cout], outs[1][:, yo:yo + cout], 1e-5)
     _close(outs[2][:, yo:yo + cout], outs[1][:, yo:yo + cout], 1e-5)
+    _close(outs[3][:, yo:yo + cout], outs[1][:, yo:yo + cout], 1e-5)
 
 
 @pytest.mark.gpu
@@ -216,13 +217,18 @@ def test_conv_input_gradient_halo(solver, cin, cout, cout_pad, dims):
     assert L.LBM_NNWeightTranspose(wd.data_ptr(), cout_pad, cin, wt.data_ptr(), cin_pad,
                                    None) == 0
     gd = _dev_bf16(g)
-    dx = torch.zeros((m, cin), dtype=torch.float32, device="cuda")
-    assert L.LBM_NNConvForward(gd.data_ptr(), cout_pad, 0, cout_pad, wt.data_ptr(), None,
-                               cin_pad, 0, None, dx.data_ptr(), cin, 0, cin, 0, *dims,
-                               None) == 0
-    assert L.LBM_NNTakeError() == 0
     ref = no.conv_dgrad(g[:, :cout], cout, w, cin, dims)
-    _close(dx.cpu().numpy(), ref, 1e-4)
+    try:
+        for path in (0, 3):
+            assert L.LBM_NNSetConvPath(path) == 0
+            dx = torch.zeros((m, cin), dtype=torch.float32, device="cuda")
+            assert L.LBM_NNConvForward(gd.data_ptr(), cout_pad, 0, cout_pad, wt.data_ptr(), None,
+                                       cin_pad, 0, None, dx.data_ptr(), cin, 0, cin, 0, *dims,
+                                       None) == 0
+            assert L.LBM_NNTakeError() == 0
+            _close(dx.cpu().numpy(), ref, 1e-4)
+    finally:
+        L.LBM_NNSetConvPath(0)
 
 
 @pytest.mark.gpu
@@ -270,4 +276,4 @@ def test_nn_argument_checks_cpu():
                                1, 8, 8, 8, None) == 1
     assert L.LBM_NNConvWeightGrad(1, 8, 0, 8, 1, 16, 12, 16, 1, 0, 1, 1 << 30, 1,
                                   1, 8, 8, 8, None) == 1
-    assert L.LBM_NNSetConvPath(3) == 1 and L.LBM_NNSetConvPath(0) == 0
+    assert L.LBM_NNSetConvPath(4) == 1 and L.LBM_NNSetConvPath(0) == 0
