@@ -15,6 +15,7 @@
 #include "lbm_nn_wgrad.cuh"
 #include "lbm_nn_wgrad_halo.cuh"
 #include "lbm_nn_zfold.cuh"
+#include "lbm_nn_wgrad_zfold.cuh"
 
 namespace lbm {
 namespace nn {
@@ -243,6 +244,39 @@ bool wgrad_halo_ok(const ConvWgradArgs &a, int nt) {
            a.d.nx % 8 == 0 && a.d.ny % 16 == 0 && a.m < (1ll << 31);
 }
 
+// Runs k_conv_wgrad_zfold over columns of tiles x z ranges, at most
+// `splits` CTAs per slice (the partial workspace holds that many); false
+// (nothing launched) when there are more columns than that.
+template <int NT>
+bool wgrad_zfold_nt(const ConvWgradArgs &a, unsigned splits, unsigned *used, cudaStream_t s,
+                    cudaError_t *e) {
+    const long long cols = (long long)a.d.nb * (a.d.ny / 16) * (a.d.nx / 8);
+    if (cols > (long long)splits || cols >= (1ll << 31)) return false;
+    long long zsegs = (long long)splits / cols;
+    if (zsegs > a.d.nz) zsegs = a.d.nz;
+    if (zsegs < 1) zsegs = 1;
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_conv_wgrad_zfold<NT>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    wz_smem_bytes<NT>());
+        if (attr == cudaSuccess)
+            attr = cudaFuncSetAttribute(k_conv_wgrad_zfold<NT>,
+                                        cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        cudaSharedmemCarveoutMaxShared);
+    });
+    if (attr != cudaSuccess) {
+        *e = attr;
+        return true;
+    }
+    k_conv_wgrad_zfold<NT><<<dim3(a.cin / 16, (unsigned)(cols * zsegs)), WZ_THREADS,
+                             wz_smem_bytes<NT>(), s>>>(a, (int)zsegs);
+    *e = cudaGetLastError();
+    *used = (unsigned)(cols * zsegs);
+    return true;
+}
+
 // Runs k_conv_wgrad_halo with at most `splits` tile ranges (the partial
 // workspace holds that many); returns the number used in *used.
 template <int NT>
@@ -401,8 +435,11 @@ cudaError_t conv_wgrad(const ConvWgradArgs &a0, int nt, unsigned splits, float *
     cudaError_t e;
     if (wgrad_halo_ok(a, nt)) {
         unsigned used = splits;
-        e = nt == 16 ? wgrad_halo_nt<16>(a, splits, &used, s)
-                     : wgrad_halo_nt<32>(a, splits, &used, s);
+        const bool zf = nt == 16 ? wgrad_zfold_nt<16>(a, splits, &used, s, &e)
+                                 : wgrad_zfold_nt<32>(a, splits, &used, s, &e);
+        if (!zf)
+            e = nt == 16 ? wgrad_halo_nt<16>(a, splits, &used, s)
+                         : wgrad_halo_nt<32>(a, splits, &used, s);
         splits = used;
     } else if (mn) {
         switch (nt) {
