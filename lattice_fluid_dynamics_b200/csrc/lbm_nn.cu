@@ -252,7 +252,10 @@ bool wgrad_zfold_nt(const ConvWgradArgs &a, unsigned splits, unsigned *used, cud
                     cudaError_t *e) {
     const long long cols = (long long)a.d.nb * (a.d.ny / 16) * (a.d.nx / 8);
     if (cols > (long long)splits || cols >= (1ll << 31)) return false;
-    long long zsegs = (long long)splits / cols;
+    // about two CTAs per SM over all slices, within the workspace and nz
+    const long long per_slice = cols * (a.cin / 16);
+    long long zsegs = (296 + per_slice - 1) / per_slice;
+    if (zsegs > (long long)splits / cols) zsegs = (long long)splits / cols;
     if (zsegs > a.d.nz) zsegs = a.d.nz;
     if (zsegs < 1) zsegs = 1;
     static std::once_flag once;
@@ -424,7 +427,8 @@ cudaError_t conv_forward(const ConvFwdArgs &a0, int nt, cudaStream_t s) {
 
 cudaError_t conv_wgrad(const ConvWgradArgs &a0, int nt, unsigned splits, float *dw,
                        int accumulate, cudaStream_t s, int cout_write, float *dbias,
-                       bool *bias_done) {
+                       bool *bias_done, unsigned max_splits) {
+    if (max_splits < splits) max_splits = splits;
     ConvWgradArgs a = a0;
     a.err = err_ptr();
     if (!a.err) return cudaErrorInvalidDevicePointer;
@@ -435,8 +439,8 @@ cudaError_t conv_wgrad(const ConvWgradArgs &a0, int nt, unsigned splits, float *
     cudaError_t e;
     if (wgrad_halo_ok(a, nt)) {
         unsigned used = splits;
-        const bool zf = nt == 16 ? wgrad_zfold_nt<16>(a, splits, &used, s, &e)
-                                 : wgrad_zfold_nt<32>(a, splits, &used, s, &e);
+        const bool zf = nt == 16 ? wgrad_zfold_nt<16>(a, max_splits, &used, s, &e)
+                                 : wgrad_zfold_nt<32>(a, max_splits, &used, s, &e);
         if (!zf)
             e = nt == 16 ? wgrad_halo_nt<16>(a, splits, &used, s)
                          : wgrad_halo_nt<32>(a, splits, &used, s);

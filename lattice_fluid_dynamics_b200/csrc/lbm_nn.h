@@ -18,9 +18,11 @@ cudaError_t conv_forward(const ConvFwdArgs &a, int nt, cudaStream_t s);
 // gradient (the sum of g over voxels) is written there too when the kernel
 // can fold it into the weight gradient (*bias_done = true); otherwise the
 // caller computes it.
+// max_splits (> splits): the partial workspace holds that many, and a kernel
+// that prefers more splits may use them.
 cudaError_t conv_wgrad(const ConvWgradArgs &a, int nt, unsigned splits, float *dw, int accumulate,
                        cudaStream_t s, int cout_write = 0, float *dbias = nullptr,
-                       bool *bias_done = nullptr);
+                       bool *bias_done = nullptr, unsigned max_splits = 0);
 cudaError_t weight_transpose(const __nv_bfloat16 *w, int cout, int cin, __nv_bfloat16 *wt,
                              int wt_rows, cudaStream_t s);
 // reads and clears the device error word of the GEMM kernels (synchronous)

@@ -752,8 +752,9 @@ bool backward(LBMWarmNet *n, const float *target_dev, int nb) {
         const Wsplit sp = wgrad_split(m, w.k_pad);
         w.chunks_per_split = sp.chunks;
         bool bias_done = false;
+        const unsigned room = (unsigned)(n->ws_bytes / ((long long)w.k_pad * nt * 4));
         if (!ok(n, conv_wgrad(w, nt, sp.splits, n->grad + n->woff[l], 0, s, kLayers[l].cout,
-                              n->grad + n->boff[l], &bias_done)))
+                              n->grad + n->boff[l], &bias_done, room)))
             return false;
         if (!bias_done) {
             const unsigned bb = nblk(m, BG_ROWS);
@@ -906,7 +907,16 @@ LBMWarmNet *LBM_WarmNetCreate(int nx, int ny, int nz, int maxBatch, unsigned see
         const int nt = nt_of(kLayers[l].cout), kp = k_pad_of(kLayers[l].cin);
         gmax = m * nt > gmax ? m * nt : gmax;
         const Wsplit sp = wgrad_split(m, kp);
-        const long long ws = (long long)sp.splits * kp * nt;
+        // layers of <= 32 output channels: room for 256 partials (at most one
+        // per 64 voxels) as well -- the z-folded weight gradient gives each
+        // column of tiles (128 at the finest level, batch 8, 64x32x32) and
+        // range of z its own
+        long long room = sp.splits;
+        if (nt <= 32) {
+            const long long cap = (m + KC - 1) / KC < 256 ? (m + KC - 1) / KC : 256;
+            room = room > cap ? room : cap;
+        }
+        const long long ws = room * kp * nt;
         wsmax = ws > wsmax ? ws : wsmax;
     }
     n->g = n->alloc<H>(gmax);
