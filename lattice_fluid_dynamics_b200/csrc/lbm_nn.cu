@@ -151,15 +151,16 @@ bool halo_shape_ok(const ConvFwdArgs &a, int nt) {
 }
 
 // The z-folded forward where there are enough columns of tiles to keep
-// every SM busy with ZF_SEG output planes per CTA and a single input slice
-// (its weights stay resident; with more slices the per-plane weight copies
-// cost more than the saved MMAs: 157 against 149 us for 48 -> 16 at
-// 8 x 64x32x32).  Path 3 takes it wherever the kernel can run.
+// every SM busy with ZF_SEG output planes per CTA and every input slice's
+// weights fit in shared memory beside the halo stages (resident for the
+// CTA's life).  Path 3 takes it wherever the kernel can run.
 bool zfold_ok(const ConvFwdArgs &a, int nt) {
     const long long cols = (long long)a.d.nb * (a.d.ny / 16) * (a.d.nx / 8);
     const long long segs = (a.d.nz + ZF_SEG - 1) / ZF_SEG;
-    return (nt == 16 || nt == 32) && cols < (1ll << 31) &&
-           (g_conv_path == 3 || (a.cin == 16 && cols * segs >= 296));
+    const int ck = a.cin / 16;
+    const int smem = nt == 16 ? zf_smem_bytes<16>(ck) : zf_smem_bytes<32>(ck);
+    return (nt == 16 || nt == 32) && cols < (1ll << 31) && smem <= 110 * 1024 &&
+           (g_conv_path == 3 || cols * segs >= 296);
 }
 
 template <int NT>
@@ -168,8 +169,7 @@ cudaError_t fwd_zfold_nt(const ConvFwdArgs &a, cudaStream_t s) {
     static cudaError_t attr = cudaSuccess;
     std::call_once(once, [] {
         attr = cudaFuncSetAttribute(k_conv_fwd_zfold<NT>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    zf_smem_bytes<NT>());
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 110 * 1024);
         if (attr == cudaSuccess)
             attr = cudaFuncSetAttribute(k_conv_fwd_zfold<NT>,
                                         cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -178,7 +178,7 @@ cudaError_t fwd_zfold_nt(const ConvFwdArgs &a, cudaStream_t s) {
     if (attr != cudaSuccess) return attr;
     const unsigned cols = (unsigned)((long long)a.d.nb * (a.d.ny / 16) * (a.d.nx / 8));
     const unsigned segs = (unsigned)((a.d.nz + ZF_SEG - 1) / ZF_SEG);
-    k_conv_fwd_zfold<NT><<<dim3(cols, segs), 128, zf_smem_bytes<NT>(), s>>>(a);
+    k_conv_fwd_zfold<NT><<<dim3(cols, segs), 128, zf_smem_bytes<NT>(a.cin / 16), s>>>(a);
     return cudaGetLastError();
 }
 

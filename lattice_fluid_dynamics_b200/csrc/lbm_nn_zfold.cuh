@@ -33,20 +33,24 @@ constexpr int ZF_HALO = 2 * ZF_PLANE;       // one 16-channel slice
 constexpr int ZF_STAGES = 3;
 constexpr int ZF_SEG = 8;                   // output planes per CTA
 
+// the weights of one 16-channel slice: [tap (dy, dx)][plane][n' = dz NT + co]
 template <int NT>
-__host__ __device__ constexpr int zf_stage_bytes() {
-    return ZF_HALO + 9 * 2 * 3 * NT * 16;
+__host__ __device__ constexpr int zf_slice_wbytes() {
+    return 9 * 2 * 3 * NT * 16;
 }
+// halo stages, then every slice's weights (copied once, resident)
 template <int NT>
-__host__ __device__ constexpr int zf_smem_bytes() {
-    return ZF_STAGES * zf_stage_bytes<NT>() + 8 * (ZF_STAGES + 1) + 16;
+__host__ __device__ constexpr int zf_smem_bytes(int ck) {
+    return ZF_STAGES * ZF_HALO + ck * zf_slice_wbytes<NT>() + 8 * (ZF_STAGES + 1) + 16;
 }
 
 template <int NT>
 __global__ void __launch_bounds__(128) k_conv_fwd_zfold(const ConvFwdArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    constexpr int S = ZF_STAGES, SB = zf_stage_bytes<NT>(), N3 = 3 * NT;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + S * SB);  // S stage barriers, 1 plane
+    constexpr int S = ZF_STAGES, SB = ZF_HALO, N3 = 3 * NT, WSL = zf_slice_wbytes<NT>();
+    const int ck = a.cin >> 4;
+    uint8_t *wsm = smem + S * SB;  // resident weights of all slices
+    uint64_t *bars = reinterpret_cast<uint64_t *>(wsm + ck * WSL);  // S stage barriers, 1 plane
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + S + 1);
     const int tid = threadIdx.x, warp = tid >> 5;
     constexpr uint32_t ncols = N3 <= 64 ? 64u : 128u;
@@ -61,7 +65,6 @@ __global__ void __launch_bounds__(128) k_conv_fwd_zfold(const ConvFwdArgs a) {
     const int ty = col % tyn;
     const int b = col / tyn;
     const int z0 = blockIdx.y * ZF_SEG, z1 = min(a.d.nz, z0 + ZF_SEG);
-    const int ck = a.cin >> 4;
     const int planes = z1 - z0 + 2;  // input planes z0 - 1 .. z1
     const int nq = z0 < z1 ? planes * ck : 0;
 
@@ -92,7 +95,7 @@ __global__ void __launch_bounds__(128) k_conv_fwd_zfold(const ConvFwdArgs a) {
     constexpr uint32_t idesc = tc::idesc_bf16_f32(128, N3);
 
     // all threads: halo plane of item q (plane q / ck, slice q % ck) into stage
-    // q % S; the weights of a slice (all of them when ck == 1, once) beside it
+    // q % S; with item 0, the weights of every slice
     auto issue = [&](int q) {
         const int p = q / ck, j = q - p * ck;
         const int zi = z0 - 1 + p;
@@ -109,15 +112,16 @@ __global__ void __launch_bounds__(128) k_conv_fwd_zfold(const ConvFwdArgs a) {
                 in ? (((long long)b * a.d.nz + zi) * a.d.ny + gy) * a.d.nx + gx : 0;
             cp_async16(st + h_soff[k], xs + vox * a.x_stride + kc * 8, in ? 16u : 0u);
         }
-        if (ck > 1 || q == 0) {
+        if (q == 0) {
             // B rows n' = dz NT + co, K = (dy, dx) tap x 16 channels
-            const uint32_t w_addr = st + ZF_HALO;
-            for (int e = tid; e < 18 * N3; e += 128) {
-                const int n = e % N3, tk = e / N3;  // tk = (dy 3 + dx) 2 + plane
+            const uint32_t w_addr = tc::smem_addr(wsm);
+            for (int e = tid; e < ck * 18 * N3; e += 128) {
+                const int js = e / (18 * N3), r = e - js * 18 * N3;
+                const int n = r % N3, tk = r / N3;  // tk = (dy 3 + dx) 2 + plane
                 const int dz = n / NT, co = n - dz * NT, t9 = tk >> 1;
                 const int tap = dz * 9 + t9;
-                cp_async16(w_addr + (tk * N3 + n) * 16,
-                           a.w + (long long)co * a.k_pad + tap * a.cin + j * 16 + (tk & 1) * 8,
+                cp_async16(w_addr + (uint32_t)(js * WSL) + (tk * N3 + n) * 16,
+                           a.w + (long long)co * a.k_pad + tap * a.cin + js * 16 + (tk & 1) * 8,
                            16u);
             }
         }
@@ -143,7 +147,7 @@ __global__ void __launch_bounds__(128) k_conv_fwd_zfold(const ConvFwdArgs a) {
         tc::fence_after_sync();
         if (tid == 0) {
             const uint32_t hb = tc::smem_addr(smem + s * SB);
-            const uint32_t wb = tc::smem_addr(smem + (ck > 1 ? s : 0) * SB) + ZF_HALO;
+            const uint32_t wb = tc::smem_addr(wsm) + (uint32_t)(j * WSL);
             const uint64_t a0 = tc::kmajor_desc(hb, ZF_PLANE, HX * 16);
             const uint64_t b0 = tc::kmajor_desc(wb, N3 * 16, 128);
 #pragma unroll
