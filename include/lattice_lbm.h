@@ -388,7 +388,7 @@ int LBM_NNTakeError(void);
  * pipelined im2col kernels elsewhere (and for every weight gradient); 1 the
  * original synchronous im2col kernels for every shape; 2 the pipelined
  * im2col kernels for every shape; 3 as 0 with the z-folded forward (three
- * z taps per MMA, coutPad 16 / 32) wherever the shape allows it, also where
+ * z taps per MMA, coutPad 16 / 32 / 48) wherever the shape allows it, also where
  * 0 would not choose it for lack of parallelism.  Process-wide; not
  * thread-safe against concurrent launches.  LBM_OK or
  * LBM_ERR_INVALID_ARGUMENT. */

@@ -158,8 +158,10 @@ bool zfold_ok(const ConvFwdArgs &a, int nt) {
     const long long cols = (long long)a.d.nb * (a.d.ny / 16) * (a.d.nx / 8);
     const long long segs = (a.d.nz + ZF_SEG - 1) / ZF_SEG;
     const int ck = a.cin / 16;
-    const int smem = nt == 16 ? zf_smem_bytes<16>(ck) : zf_smem_bytes<32>(ck);
-    return (nt == 16 || nt == 32) && cols < (1ll << 31) && smem <= 110 * 1024 &&
+    const int smem = nt == 16   ? zf_smem_bytes<16>(ck)
+                     : nt == 32 ? zf_smem_bytes<32>(ck)
+                                : zf_smem_bytes<48>(ck);
+    return (nt == 16 || nt == 32 || nt == 48) && cols < (1ll << 31) && smem <= 110 * 1024 &&
            (g_conv_path == 3 || cols * segs >= 296);
 }
 
@@ -404,7 +406,10 @@ cudaError_t conv_forward(const ConvFwdArgs &a0, int nt, cudaStream_t s) {
     a.err = err_ptr();
     if (!a.err) return cudaErrorInvalidDevicePointer;
     if (halo_shape_ok(a, nt)) {
-        if (zfold_ok(a, nt)) return nt == 16 ? fwd_zfold_nt<16>(a, s) : fwd_zfold_nt<32>(a, s);
+        if (zfold_ok(a, nt))
+            return nt == 16   ? fwd_zfold_nt<16>(a, s)
+                   : nt == 32 ? fwd_zfold_nt<32>(a, s)
+                              : fwd_zfold_nt<48>(a, s);
         switch (nt) {
             case 16: return fwd_halo_nt<16>(a, s);
             case 32: return fwd_halo_nt<32>(a, s);

@@ -1,6 +1,6 @@
 // Forward convolution with the three z taps folded into N, for the halo
 // shapes (input channels a multiple of 16, NX a multiple of 8, NY of 16)
-// with NT <= 32 output channels.
+// with NT = 16, 32 or 48 output channels (N = 3 NT <= 256).
 //
 //     y[z] = Q_0[z - 1] + Q_1[z] + Q_2[z + 1],
 //     Q_dz[z'][v][co] = sum over (dy, dx, c) of x[z'][v + (dx, dy)][c] W[co][(dz, dy, dx, c)]
@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(128) k_conv_fwd_zfold(const ConvFwdArgs a) {
     uint64_t *bars = reinterpret_cast<uint64_t *>(wsm + ck * WSL);  // S stage barriers, 1 plane
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + S + 1);
     const int tid = threadIdx.x, warp = tid >> 5;
-    constexpr uint32_t ncols = N3 <= 64 ? 64u : 128u;
+    constexpr uint32_t ncols = N3 <= 64 ? 64u : N3 <= 128 ? 128u : 256u;
     const uint32_t bar_acc = tc::smem_addr(&bars[S]);
     auto bar_stage = [&](int s) { return tc::smem_addr(&bars[s]); };
 
