@@ -365,10 +365,21 @@ __global__ void k_wgrad_reduce(const float *__restrict__ partial, int splits, in
     const int rows = k_real + (dbias ? 1 : 0);
     const bool live = o < (long long)cout * rows;
     const int k = live ? (int)(o / cout) : 0, n = live ? (int)(o - (long long)k * cout) : 0;
+    // eight independent loads in flight per thread, summed in split order
     float s = 0.f;
-    if (live)
-        for (int p = r; p < splits; p += WR_GROUPS)
-            s += partial[((long long)p * k_pad + k) * nt + n];
+    if (live) {
+        const float *src = partial + (long long)k * nt + n;
+        const long long stride = (long long)k_pad * nt;
+        int p = r;
+        for (; p + 7 * WR_GROUPS < splits; p += 8 * WR_GROUPS) {
+            float v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) v[u] = src[(long long)(p + u * WR_GROUPS) * stride];
+#pragma unroll
+            for (int u = 0; u < 8; u++) s += v[u];
+        }
+        for (; p < splits; p += WR_GROUPS) s += src[(long long)p * stride];
+    }
     part[r][ol] = s;
     __syncthreads();
     if (r == 0 && live) {
