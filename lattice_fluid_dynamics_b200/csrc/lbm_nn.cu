@@ -150,19 +150,29 @@ bool halo_shape_ok(const ConvFwdArgs &a, int nt) {
            (long long)a.d.nb * a.d.nz * (a.d.ny / 16) * (a.d.nx / 8) < (1ll << 31);
 }
 
+// Output planes per CTA of the z-folded forward: ZF_SEG, fewer (down to 2)
+// where that leaves fewer than ~2 CTAs per SM.
+int zfold_seg(const ConvFwdArgs &a) {
+    const long long cols = (long long)a.d.nb * (a.d.ny / 16) * (a.d.nx / 8);
+    int seg = ZF_SEG;
+    while (seg > 2 && cols * ((a.d.nz + seg - 1) / seg) < 296) seg /= 2;
+    return seg;
+}
+
 // The z-folded forward where there are enough columns of tiles to keep
-// every SM busy with ZF_SEG output planes per CTA and every input slice's
-// weights fit in shared memory beside the halo stages (resident for the
-// CTA's life).  Path 3 takes it wherever the kernel can run.
+// every SM busy with at least 2 output planes per CTA and every input
+// slice's weights fit in shared memory beside the halo stages (resident for
+// the CTA's life).  Path 3 takes it wherever the kernel can run.
 bool zfold_ok(const ConvFwdArgs &a, int nt) {
     const long long cols = (long long)a.d.nb * (a.d.ny / 16) * (a.d.nx / 8);
-    const long long segs = (a.d.nz + ZF_SEG - 1) / ZF_SEG;
+    const int seg = zfold_seg(a);
+    const long long segs = (a.d.nz + seg - 1) / seg;
     const int ck = a.cin / 16;
     const int smem = nt == 16   ? zf_smem_bytes<16>(ck)
                      : nt == 32 ? zf_smem_bytes<32>(ck)
                                 : zf_smem_bytes<48>(ck);
     return (nt == 16 || nt == 32 || nt == 48) && cols < (1ll << 31) && smem <= 110 * 1024 &&
-           (g_conv_path == 3 || cols * segs >= 296);
+           (g_conv_path == 3 || cols * segs >= 200);
 }
 
 template <int NT>
@@ -179,8 +189,9 @@ cudaError_t fwd_zfold_nt(const ConvFwdArgs &a, cudaStream_t s) {
     });
     if (attr != cudaSuccess) return attr;
     const unsigned cols = (unsigned)((long long)a.d.nb * (a.d.ny / 16) * (a.d.nx / 8));
-    const unsigned segs = (unsigned)((a.d.nz + ZF_SEG - 1) / ZF_SEG);
-    k_conv_fwd_zfold<NT><<<dim3(cols, segs), 128, zf_smem_bytes<NT>(a.cin / 16), s>>>(a);
+    const int seg = zfold_seg(a);
+    const unsigned segs = (unsigned)((a.d.nz + seg - 1) / seg);
+    k_conv_fwd_zfold<NT><<<dim3(cols, segs), 128, zf_smem_bytes<NT>(a.cin / 16), s>>>(a, seg);
     return cudaGetLastError();
 }
 

@@ -5,7 +5,8 @@
 //     y[z] = Q_0[z - 1] + Q_1[z] + Q_2[z + 1],
 //     Q_dz[z'][v][co] = sum over (dy, dx, c) of x[z'][v + (dx, dy)][c] W[co][(dz, dy, dx, c)]
 //
-// One CTA walks a column of 8 x 16 tiles through a range of z: for each
+// One CTA walks a column of 8 x 16 tiles through a range of `seg` output
+// planes (input planes z0 - 1 .. z0 + seg, the ends read twice): for each
 // input plane z' it copies the plane's 10 x 18 halo (per 16-channel slice,
 // two 8-channel planes, as k_conv_fwd_halo) and issues, per (dy, dx) tap,
 // one MMA of M = 128 voxels, N = 3 NT (the three dz blocks of output
@@ -31,7 +32,7 @@ constexpr int ZF_PVOX = HX * HY;            // 180 voxels of one halo plane
 constexpr int ZF_PLANE = ZF_PVOX * 16;      // one 8-channel plane: 2,880 B
 constexpr int ZF_HALO = 2 * ZF_PLANE;       // one 16-channel slice
 constexpr int ZF_STAGES = 3;
-constexpr int ZF_SEG = 8;                   // output planes per CTA
+constexpr int ZF_SEG = 8;                   // output planes per CTA, at most
 
 // the weights of one 16-channel slice: [tap (dy, dx)][plane][n' = dz NT + co]
 template <int NT>
@@ -45,7 +46,7 @@ __host__ __device__ constexpr int zf_smem_bytes(int ck) {
 }
 
 template <int NT>
-__global__ void __launch_bounds__(128) k_conv_fwd_zfold(const ConvFwdArgs a) {
+__global__ void __launch_bounds__(128) k_conv_fwd_zfold(const ConvFwdArgs a, int seg) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int S = ZF_STAGES, SB = ZF_HALO, N3 = 3 * NT, WSL = zf_slice_wbytes<NT>();
     const int ck = a.cin >> 4;
@@ -64,7 +65,7 @@ __global__ void __launch_bounds__(128) k_conv_fwd_zfold(const ConvFwdArgs a) {
     col /= txn;
     const int ty = col % tyn;
     const int b = col / tyn;
-    const int z0 = blockIdx.y * ZF_SEG, z1 = min(a.d.nz, z0 + ZF_SEG);
+    const int z0 = blockIdx.y * seg, z1 = min(a.d.nz, z0 + seg);
     const int planes = z1 - z0 + 2;  // input planes z0 - 1 .. z1
     const int nq = z0 < z1 ? planes * ck : 0;
 
